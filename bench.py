@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Benchmark of the continuous Frechet distance engine on B200.
+
+One step is one full solve (endpoint bound, DFD, VE-FD, epsilon search to 2^-33 relative,
+i.e. within 1e-9 of the FP64 result) of the long-pair workload: two 200,000-point 3D
+robot-like paths (Catmull-Rom through 2,000 waypoints U[-100,100]^3, the second path under
+a 20-knot monotone time warp plus N(0, 0.1^2) noise, seed 1), 4.0e10 free-space cells per
+decision.  Inputs are synthetic and seeded (the reference ships no data).
+
+  value : FD solves/s with both curves resident in HBM (rfd_distance on device pointers)
+  e2e   : the same through the C ABI with host buffers (H2D copy, solve, D2H result)
+  roofline : the dominant phase kernel against the measured FP64 FMA peak
+  cpu_baseline : the CPU oracle (dense FP64 restatement, OpenMP) on a bounded sample,
+                 extrapolated to the full pair
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun every rank solves the same pair (the path does not shard: replicas only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FD solves/s and free-space cells/s at <=1e-9 rel err vs FP64 plain GPU form"
+WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-100,100]^3, "
+            "20-knot time warp, noise 0.1, seed 1); FD to 2^-33 relative")
+# algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
+# DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
+FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3, "vefd": lambda d: 24 * d + 2,
+                  "search": lambda d: 12 * d + 22}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=12000,
+                    help="points per curve of the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [v for v in sm if v > 0.5 * (mx or 1)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload():
+    import robotfd_b200 as rfd
+    return rfd.gen_config(1)[0]
+
+
+def cpu_sample(P, Q, m, probes):
+    """Dense CPU oracle on the first m points of each curve: DFD, VE-FD and one decision,
+    timed; the rates extrapolate to one solve of the full pair with `probes` decisions."""
+    import oracle
+    threads = oracle.max_threads()
+    Ps, Qs = np.ascontiguousarray(P[:m]), np.ascontiguousarray(Q[:m])
+    lb = oracle.endpoint(Ps, Qs)
+    t0 = time.perf_counter()
+    dsq = oracle.dfd_sq(Ps, Qs, threads)
+    t1 = time.perf_counter()
+    vsq = oracle.vefd_sq(Ps, Qs, lb, threads)
+    t2 = time.perf_counter()
+    oracle.decide(Ps, Qs, 0.5 * (np.sqrt(dsq) + np.sqrt(vsq)), threads)
+    t3 = time.perf_counter()
+    pts, cells = m * m, (m - 1) * (m - 1)
+    r_dfd, r_ve, r_dec = pts / (t1 - t0), cells / (t2 - t1), cells / (t3 - t2)
+    n1, n2 = len(P), len(Q)
+    sec = n1 * n2 / r_dfd + (n1 - 1) * (n2 - 1) * (1 / r_ve + probes / r_dec)
+    return {
+        "value": 1.0 / sec, "unit": "solves/s", "cores": threads, "kind": "port",
+        "sample": (f"oracle (dense FP64, OpenMP {threads} threads): DFD, VE-FD and one decision "
+                   f"on the first {m} points of each curve ({t3 - t0:.1f} s), extrapolated to "
+                   f"the full pair with {probes} decisions"),
+        "cells_per_s": {"dfd": r_dfd, "vefd": r_ve, "decision": r_dec},
+    }
+
+
+def reference_arm(args):
+    """CPU implementation of the path (the oracle port: the reference has no CPU path)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    P, Q = workload()
+    probes = 37  # decisions of this workload's solve at 2^-33 (identical decisions as the GPU)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_sample(P, Q, args.cpu_sample, probes)
+        if k >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.median(vals)
+    r["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "cpu"},
+            "cpu_baseline": r,
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import robotfd_b200 as rfd
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    ctx = rfd.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    P, Q = workload()
+    n1, n2, d = len(P), len(Q), P.shape[1]
+    dP = torch.from_numpy(P).cuda()
+    dQ = torch.from_numpy(Q).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step_dev():
+        return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True)
+
+    def step_host():
+        return ctx.distance(P, Q, precise=True)
+
+    def timed(fn, k, tag):
+        times, res = [], None
+        for _ in range(k):
+            flush.fill_(1)  # L2 flush outside the event pair
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = fn()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times, res
+
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ctx.phase_times(enable=1)
+    clocks = Clocks(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    times, res = timed(step_dev, args.steps, "value")
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    phases = ctx.phase_times(enable=0)
+    total_ms = sum(times)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+
+    # e2e: host buffers through the C ABI, copies inside the timed region
+    ctx.phase_times(enable=1)
+    etimes, eres = timed(step_host, args.steps, "e2e")
+    ephase = ctx.phase_times(enable=0)
+    e_ms = sum(etimes)
+    if dist:
+        t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = world * args.steps / (e_ms / 1e3)
+    assert eres["distance"] == res["distance"], "host and device inputs disagree"
+
+    peak = ctx.fp64_peak()
+    calls = max(phases["calls"], 1)
+    ph_ms = {k: phases[k + "_ms"] / calls for k in ("dfd", "vefd", "search")}
+    cells = {
+        "dfd": n1 * n2,
+        "vefd": res["cells_vefd"],
+        "search": res["cells_evaluated"],
+    }
+    dom = max(ph_ms, key=ph_ms.get)
+    flops = cells[dom] * FLOPS_PER_CELL[dom](d)
+    achieved = flops / (ph_ms[dom] * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(dom)
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n1": n1, "n2": n2, "dims": d,
+                   "stop": "ub-lb <= 2^-33 ub", "parallelism": f"replicas x{world}",
+                   "l2": "flushed before every step (256 MiB write outside the timed events)"},
+        "fd": res["distance"],
+        "probes": res["probes"],
+        "free_space_cells_per_s": {
+            "nominal": res["cells_nominal"] / (ph_ms["search"] * 1e-3),
+            "evaluated": res["cells_evaluated"] / (ph_ms["search"] * 1e-3),
+            "evaluated_fraction": res["cells_evaluated"] / max(res["cells_nominal"], 1),
+        },
+        "bounds_cells_per_s": {"dfd": n1 * n2 / (ph_ms["dfd"] * 1e-3),
+                               "vefd_nominal": (n1 - 1) * (n2 - 1) / (ph_ms["vefd"] * 1e-3),
+                               "vefd_evaluated": res["cells_vefd"] / (ph_ms["vefd"] * 1e-3)},
+        "phase_ms": ph_ms,
+        "roofline": {"bound": "fp64", "kernel": f"wave_kernel<{dom}>", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "peak_source": "measured FP64 FMA throughput (rfd_fp64_peak), this GPU",
+                     "flops_per_cell": FLOPS_PER_CELL[dom](d), "cells": cells[dom]},
+        "e2e": {"value": e2e_value, "unit": "solves/s",
+                "h2d_bytes_per_step": ephase["h2d_bytes"] / max(ephase["calls"], 1),
+                "d2h_bytes_per_step": ephase["d2h_bytes"] / max(ephase["calls"], 1)},
+        "gpu_launches": int(phases["launches"]),
+        "clocks": clk,
+    }
+    if rank == 0:
+        if world == 1:
+            line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, res["probes"])
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * rfd.h - C ABI of the B200 continuous Frechet distance engine (librfd.so).
+ *
+ * Curves are caller-owned arrays of doubles in interleaved [n][dims] layout
+ * (dims 2 or 3), the same flattening the reference performs in
+ * Cuda_intersection::Cuda_intersection (src/intersection_algorithm_in_parallel.cu:42-51).
+ * Every function returns an rfd_status code; nothing prints.  A context owns one
+ * CUDA device, one stream and a cached device workspace; calls on one context
+ * are serialised by the caller, distinct contexts may be used from distinct
+ * threads.
+ */
+#ifndef RFD_H
+#define RFD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RFD_ABI_VERSION 1
+#define RFD_MAX_PROBES 200
+
+/* Status codes (the reference prints CUDA errors and carries on; this ABI reports them). */
+enum rfd_status {
+  RFD_OK = 0,
+  RFD_ERR_ARG = 1,      /* null pointer, dims not 2/3, empty curve, bad option */
+  RFD_ERR_CUDA = 2,     /* a CUDA runtime call failed (message: rfd_last_error) */
+  RFD_ERR_NOMEM = 3,    /* device or pinned host allocation failed */
+  RFD_ERR_TIMEOUT = 4,  /* a bounded inter-warp wait expired; results are not valid */
+  RFD_ERR_NODEV = 5,    /* no CUDA device, or the library was built without one */
+  RFD_ERR_INTERNAL = 6,
+  RFD_ERR_LIMIT = 7     /* a size exceeds a stated maximum */
+};
+
+/* Stop rule of the epsilon search. */
+enum rfd_stop {
+  RFD_STOP_ABS = 0, /* while (ub - lb > tol): the reference rule, tol = FLT_EPSILON
+                       (src/frechet.cpp:41, src/compute_distance_wrapper.cpp:6) */
+  RFD_STOP_REL = 1  /* while (ub - lb > tol * ub): relative rule for the 1e-9 metric */
+};
+
+enum rfd_memory { RFD_MEM_HOST = 0, RFD_MEM_DEVICE = 1 };
+
+enum rfd_precision {
+  RFD_PREC_FP64 = 0,       /* every interval in FP64 */
+  RFD_PREC_FP32_FILTER = 1 /* FP32 classification with a proven margin, FP64 recheck */
+};
+
+/* Result flags. */
+enum rfd_flag {
+  RFD_FLAG_VEFD_SKIPPED = 1,   /* reference quirk: (int)(n1*n2) <= 10000, lb = endpoint bound */
+  RFD_FLAG_LB_GT_UB = 2,       /* VE-FD came out above DFD (the reference asserts here) */
+  RFD_FLAG_MAX_PROBES = 4,     /* stopped by max_probes */
+  RFD_FLAG_STALLED = 8,        /* (lb+ub)/2 equals lb or ub: no further progress in doubles */
+  RFD_FLAG_VEFD_DENSE = 16,    /* VE-FD pruning bound was too tight, recomputed without pruning */
+  RFD_FLAG_BRACKET_USED = 32,  /* a proposed bracket was verified and used */
+  RFD_FLAG_BRACKET_WIDENED = 64, /* a proposed bracket failed verification and was widened */
+  RFD_FLAG_DEGENERATE = 128    /* a curve of one point: closed form used */
+};
+
+typedef struct rfd_options {
+  int32_t stop_mode;        /* enum rfd_stop */
+  int32_t reference_quirks; /* 1: reproduce the reference's VE-FD launch rule
+                               (src/intersection_algorithm_in_parallel.cu:1343) */
+  double tol;               /* see rfd_stop */
+  int32_t max_probes;       /* cap on decisions per pair, <= RFD_MAX_PROBES */
+  int32_t dense;            /* 1: evaluate every cell (no dead-region skipping) */
+  int32_t precision;        /* enum rfd_precision */
+  int32_t memory;           /* where curve pointers live: enum rfd_memory */
+  const double* bracket;    /* optional, 2 doubles per pair: proposed [lo, hi] containing the
+                               distance; verified by two decisions, widened on failure */
+} rfd_options;
+
+typedef struct rfd_result {
+  double distance;          /* (lb + ub) / 2 at the stop (src/frechet.cpp:63) */
+  double dfd;               /* discrete Frechet distance: the initial upper bound */
+  double vefd;              /* vertex-edge Frechet distance: the initial lower bound */
+  double endpoint;          /* max(|p0 - q0|, |pn - qm|) (src/frechet.cpp:30) */
+  double lb, ub;            /* final bracket */
+  int64_t cells_nominal;    /* sum over decisions of (n1-1)(n2-1) */
+  int64_t cells_evaluated;  /* decision cells the kernels actually evaluated */
+  int64_t cells_fp64;       /* of those, cells whose intervals were computed in FP64 */
+  int64_t cells_vefd;       /* VE-FD cells evaluated (of (n1-1)(n2-1) per pass) */
+  int32_t probes;           /* decisions made */
+  int32_t flags;            /* enum rfd_flag */
+} rfd_result;
+
+typedef struct rfd_context rfd_context;
+
+/* ---- library ---- */
+int32_t rfd_abi_version(void);
+const char* rfd_status_string(int32_t status);
+/* Message of the last failing call on this thread ("" when none). */
+const char* rfd_last_error(void);
+
+/* Options of the reference (ABS stop at FLT_EPSILON, quirks on) when precise == 0,
+   else the relative rule at tol = 2^-33 with quirks off. */
+void rfd_options_init(rfd_options* opt, int32_t precise);
+
+/* ---- context ---- */
+int32_t rfd_context_create(int32_t device, rfd_context** out);
+int32_t rfd_context_destroy(rfd_context* ctx);
+/* Use a caller stream (cudaStream_t) instead of the context's own; NULL restores it. */
+int32_t rfd_context_set_stream(rfd_context* ctx, void* stream);
+/* Phase timing with CUDA events on the context's stream (off by default; no reference
+   counterpart - the reference prints host wall times, src/frechet.cpp:65-71).
+   enable: 1 on, 0 off, -1 leave as is.  When out != NULL it receives, for the calls since
+   the previous query, out[0] = ms in constants + DFD, out[1] = ms in VE-FD, out[2] = ms in
+   decisions, out[3] = calls, out[4] = kernel launches, out[5] = bytes copied host to device,
+   out[6] = bytes copied device to host; the counters are then reset. */
+int32_t rfd_context_phase_times(rfd_context* ctx, int32_t enable, double* out);
+
+/* Measured FP64 fused multiply-add throughput of the context's device in TFLOP/s (2 flops
+   per FMA): independent FMA chains at full occupancy, timed with CUDA events.  The roofline
+   denominator for the FP64 wavefront kernels (no reference counterpart). */
+int32_t rfd_fp64_peak(rfd_context* ctx, double* tflops);
+
+/* ---- the hot path ---- */
+
+/* One continuous Frechet distance: endpoint bound, DFD and VE-FD bracket, epsilon search.
+   Replaces compute_distance_parallel (include/wrapper.hpp:4, src/compute_distance_wrapper.cpp:8)
+   and Frechet::Continuous::distance_cuda (include/frechet.hpp:14, src/frechet.cpp:18). */
+int32_t rfd_distance(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                     int32_t dims, const rfd_options* opt, rfd_result* out);
+
+/* Many pairs in one persistent launch sequence (no reference counterpart: the reference
+   solves one pair per call).  c1s/c2s are arrays of npairs curve pointers; dims may differ
+   per pair.  Results are written to out[0..npairs). */
+int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s,
+                           const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
+                           const int32_t* dims, const rfd_options* opt, rfd_result* out);
+
+/* The two bounds.  *vefd is read as the endpoint lower bound that seeds VE-FD and
+   overwritten with VE-FD (left unchanged when the reference rule skips it and
+   reference_quirks != 0).  Replaces Cuda_intersection::Bound_call_gpu
+   (include/intersection_algorithm_in_parallel.hpp:26, src/intersection_algorithm_in_parallel.cu:1258). */
+int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                   int32_t dims, int32_t reference_quirks, int32_t dense, double* dfd, double* vefd);
+
+/* One free-space reachability decision at distance `radius`: *reachable = 1 when the
+   propagated right interval of the last cell ends at 1.0.  *right_ub receives that
+   value (may be NULL).  Replaces Cuda_intersection::intersection_interval_call_gpu
+   (include/intersection_algorithm_in_parallel.hpp:19, src/intersection_algorithm_in_parallel.cu:1398). */
+int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                   int32_t dims, double radius, int32_t dense, int32_t* reachable, double* right_ub);
+
+/* ---- loader ----
+   Text curve loader: one point per line, comma separated, consecutive duplicates dropped.
+   Replaces txtLoader2 / txtLoader3 (include/txtReader.hpp:6, :48).  On success *out is a
+   malloc'd [*n][dims] array released with rfd_free. */
+int32_t rfd_load_txt(const char* path, int32_t dims, int32_t start, int32_t limit, double** out,
+                     int64_t* n);
+void rfd_free(void* p);
+
+/* ---- synthetic workloads (seeded; see robotfd_b200/csrc/rfd_gen.cpp) ---- */
+int32_t rfd_gen_pair(int32_t style, int32_t dims, int64_t n1, int64_t n2, double scale, double noise,
+                     uint64_t seed, uint64_t stream, double* P, int64_t* out_n1, double* Q,
+                     int64_t* out_n2);
+int32_t rfd_gen_batch_spec(int32_t config, int64_t npairs, uint64_t seed, int32_t* dims, int64_t* n1s,
+                           int64_t* n2s, int32_t* styles, double* scales, double* noises);
+
+/* ---- search state machine (host-callable copy of the device logic, for tests) ----
+   Applies one decision outcome to a bracket search and proposes the next probe.
+   state[0..5] = {lb, ub, lo, hi, tol, unused}, istate[0..3] = {mode, probes, max_probes, flags},
+   stop_mode as in rfd_options.  Returns 1 and *next_eps when another probe is due. */
+int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32_t have_outcome,
+                        double eps, int32_t reachable, double* next_eps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RFD_H */

@@ -1,0 +1,126 @@
+"""CPU oracle for the continuous Frechet distance path (TEST INFRASTRUCTURE ONLY).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+may import this package, as the checker or the timed CPU baseline; the product
+(``robotfd_b200``) never calls it.  The C source ``rfd_oracle.c`` restates the
+reference's DFD, VE-FD and fused-decision cells and its epsilon search (file:line
+citations in its header).  Parity is pinned by mathematical known-answer tests and by
+outputs of the reference's own GPU code run on the same inputs (``tests/golden``).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        i64 = ctypes.c_int64
+        L.rfd_oracle_endpoint.restype = ctypes.c_double
+        L.rfd_oracle_endpoint.argtypes = [_dp, i64, _dp, i64, ctypes.c_int]
+        L.rfd_oracle_dfd_sq.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_int, _dp]
+        L.rfd_oracle_vefd_sq.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, _dp]
+        L.rfd_oracle_decide.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, _dp]
+        L.rfd_oracle_distance.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _dp, _ip, _dp, _ip]
+        L.rfd_oracle_max_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _arr(c):
+    a = np.ascontiguousarray(c, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] not in (2, 3):
+        raise ValueError("curve must be an (n, 2) or (n, 3) array")
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def max_threads():
+    return lib().rfd_oracle_max_threads()
+
+
+def endpoint(P, Q):
+    P, Q = _arr(P), _arr(Q)
+    return lib().rfd_oracle_endpoint(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1])
+
+
+def dfd_sq(P, Q, threads=1):
+    P, Q = _arr(P), _arr(Q)
+    out = ctypes.c_double()
+    rc = lib().rfd_oracle_dfd_sq(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], threads,
+                                 ctypes.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle dfd failed ({rc})")
+    return out.value
+
+
+def vefd_sq(P, Q, lb, threads=1):
+    P, Q = _arr(P), _arr(Q)
+    out = ctypes.c_double()
+    rc = lib().rfd_oracle_vefd_sq(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], lb, threads,
+                                  ctypes.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle vefd failed ({rc})")
+    return out.value
+
+
+def decide(P, Q, radius, threads=1):
+    """Returns (reachable, propagated right UB of the last cell)."""
+    P, Q = _arr(P), _arr(Q)
+    out = ctypes.c_double()
+    rc = lib().rfd_oracle_decide(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], radius, threads,
+                                 ctypes.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle decide failed ({rc})")
+    return out.value == 1.0, out.value
+
+
+FLT_EPSILON = float(np.finfo(np.float32).eps)
+REL_TOL = 2.0 ** -33
+
+
+def distance(P, Q, stop_mode=0, tol=None, quirks=True, max_probes=200, threads=1):
+    """Full search.  stop_mode 0 is the reference rule (ub-lb > FLT_EPSILON)."""
+    P, Q = _arr(P), _arr(Q)
+    if tol is None:
+        tol = FLT_EPSILON if stop_mode == 0 else REL_TOL
+    out = (ctypes.c_double * 6)()
+    probes = ctypes.c_int()
+    log_eps = (ctypes.c_double * max(1, max_probes))()
+    log_dec = (ctypes.c_int * max(1, max_probes))()
+    rc = lib().rfd_oracle_distance(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], stop_mode, tol,
+                                   int(bool(quirks)), max_probes, threads, out,
+                                   ctypes.byref(probes), log_eps, log_dec)
+    if rc:
+        raise RuntimeError(f"oracle distance failed ({rc})")
+    n = probes.value
+    return {
+        "distance": out[0], "dfd": out[1], "vefd": out[2], "endpoint": out[3],
+        "lb": out[4], "ub": out[5], "probes": n,
+        "probe_eps": [log_eps[k] for k in range(n)],
+        "probe_dec": [bool(log_dec[k]) for k in range(n)],
+    }

@@ -1,0 +1,385 @@
+"""B200-native continuous Frechet distance engine (Python binding of librfd.so).
+
+The product is the C ABI in ``include/rfd.h`` implemented by ``librfd.so`` (CUDA kernels
+for sm_100a plus a C++ drop-in of the reference's ``compute_distance_parallel`` /
+``Curve`` / ``txtLoaderX`` API).  This module binds it with ctypes.  There is no CPU
+fallback: every distance, bound and decision runs the CUDA kernels, and a missing
+library or device raises.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_CSRC = os.path.join(_HERE, "csrc")
+LIB_PATH = os.path.join(_HERE, "librfd.so")
+FD_PATH = os.path.join(_HERE, "fd")
+
+RFD_OK = 0
+RFD_ERR_ARG = 1
+RFD_ERR_CUDA = 2
+RFD_ERR_NOMEM = 3
+RFD_ERR_TIMEOUT = 4
+RFD_ERR_NODEV = 5
+RFD_ERR_INTERNAL = 6
+RFD_ERR_LIMIT = 7
+
+RFD_STOP_ABS = 0
+RFD_STOP_REL = 1
+RFD_MEM_HOST = 0
+RFD_MEM_DEVICE = 1
+RFD_PREC_FP64 = 0
+RFD_PREC_FP32_FILTER = 1
+
+FLAG_VEFD_SKIPPED = 1
+FLAG_LB_GT_UB = 2
+FLAG_MAX_PROBES = 4
+FLAG_STALLED = 8
+FLAG_VEFD_DENSE = 16
+FLAG_BRACKET_USED = 32
+FLAG_BRACKET_WIDENED = 64
+FLAG_DEGENERATE = 128
+
+FLT_EPSILON = float(np.finfo(np.float32).eps)
+REL_TOL = 2.0 ** -33
+
+# Every symbol include/rfd.h declares.
+EXPORTS = (
+    "rfd_abi_version", "rfd_status_string", "rfd_last_error", "rfd_options_init",
+    "rfd_context_create", "rfd_context_destroy", "rfd_context_set_stream",
+    "rfd_context_phase_times", "rfd_fp64_peak", "rfd_distance",
+    "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_load_txt", "rfd_free",
+    "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step",
+)
+
+
+class RfdError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"rfd status {code} ({_status_name(code)}): {msg}")
+        self.code = code
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("stop_mode", ctypes.c_int32),
+        ("reference_quirks", ctypes.c_int32),
+        ("tol", ctypes.c_double),
+        ("max_probes", ctypes.c_int32),
+        ("dense", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("memory", ctypes.c_int32),
+        ("bracket", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("distance", ctypes.c_double),
+        ("dfd", ctypes.c_double),
+        ("vefd", ctypes.c_double),
+        ("endpoint", ctypes.c_double),
+        ("lb", ctypes.c_double),
+        ("ub", ctypes.c_double),
+        ("cells_nominal", ctypes.c_int64),
+        ("cells_evaluated", ctypes.c_int64),
+        ("cells_fp64", ctypes.c_int64),
+        ("cells_vefd", ctypes.c_int64),
+        ("probes", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_LIB = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+def build(jobs=8):
+    """Compile librfd.so and the fd CLI in-tree for sm_100a (nvcc cross-compiles)."""
+    subprocess.run(["make", "-s", "-j", str(jobs), "-C", _CSRC], check=True)
+
+
+def lib():
+    """Loads librfd.so; raises when it has not been built (no fallback path exists)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RfdError(RFD_ERR_NODEV, f"{LIB_PATH} is missing: run robotfd_b200.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    i32, i64, dbl, vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+    L.rfd_abi_version.restype = i32
+    L.rfd_status_string.restype = ctypes.c_char_p
+    L.rfd_status_string.argtypes = [i32]
+    L.rfd_last_error.restype = ctypes.c_char_p
+    L.rfd_options_init.argtypes = [ctypes.POINTER(Options), i32]
+    L.rfd_options_init.restype = None
+    L.rfd_context_create.argtypes = [i32, ctypes.POINTER(vp)]
+    L.rfd_context_create.restype = i32
+    L.rfd_context_destroy.argtypes = [vp]
+    L.rfd_context_destroy.restype = i32
+    L.rfd_context_set_stream.argtypes = [vp, vp]
+    L.rfd_context_set_stream.restype = i32
+    L.rfd_context_phase_times.argtypes = [vp, i32, _dp]
+    L.rfd_context_phase_times.restype = i32
+    L.rfd_fp64_peak.argtypes = [vp, _dp]
+    L.rfd_fp64_peak.restype = i32
+    L.rfd_distance.argtypes = [vp, vp, i64, vp, i64, i32, ctypes.POINTER(Options),
+                               ctypes.POINTER(Result)]
+    L.rfd_distance.restype = i32
+    L.rfd_distance_batch.argtypes = [vp, i64, ctypes.POINTER(vp), _i64p, ctypes.POINTER(vp), _i64p,
+                                     _i32p, ctypes.POINTER(Options), ctypes.POINTER(Result)]
+    L.rfd_distance_batch.restype = i32
+    L.rfd_bounds.argtypes = [vp, vp, i64, vp, i64, i32, i32, i32, _dp, _dp]
+    L.rfd_bounds.restype = i32
+    L.rfd_decide.argtypes = [vp, vp, i64, vp, i64, i32, dbl, i32, _i32p, _dp]
+    L.rfd_decide.restype = i32
+    L.rfd_load_txt.argtypes = [ctypes.c_char_p, i32, i32, i32, ctypes.POINTER(_dp), _i64p]
+    L.rfd_load_txt.restype = i32
+    L.rfd_free.argtypes = [vp]
+    L.rfd_free.restype = None
+    L.rfd_gen_pair.argtypes = [i32, i32, i64, i64, dbl, dbl, ctypes.c_uint64, ctypes.c_uint64,
+                               _dp, _i64p, _dp, _i64p]
+    L.rfd_gen_pair.restype = i32
+    L.rfd_gen_batch_spec.argtypes = [i32, i64, ctypes.c_uint64, _i32p, _i64p, _i64p, _i32p, _dp, _dp]
+    L.rfd_gen_batch_spec.restype = i32
+    L.rfd_search_step.argtypes = [_dp, _i32p, i32, i32, dbl, i32, _dp]
+    L.rfd_search_step.restype = i32
+    _LIB = L
+    return L
+
+
+def _status_name(code):
+    try:
+        return lib().rfd_status_string(code).decode()
+    except Exception:  # library not loadable: plain code
+        return str(code)
+
+
+def _check(code):
+    if code != RFD_OK:
+        raise RfdError(code, lib().rfd_last_error().decode())
+
+
+def _curve(c):
+    a = np.ascontiguousarray(c, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] not in (2, 3) or a.shape[0] < 1:
+        raise ValueError("a curve is a non-empty (n, 2) or (n, 3) array")
+    return a
+
+
+def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
+            precision=RFD_PREC_FP64):
+    o = Options()
+    lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
+    o.dense = int(bool(dense))
+    o.max_probes = int(max_probes)
+    o.memory = memory
+    o.precision = precision
+    if tol is not None:
+        o.tol = float(tol)
+    if quirks is not None:
+        o.reference_quirks = int(bool(quirks))
+    return o
+
+
+class Context:
+    """One CUDA device, one stream, a cached device workspace (rfd_context)."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().rfd_context_create(int(device), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().rfd_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        _check(lib().rfd_context_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def phase_times(self, enable=-1):
+        """Per-phase device ms since the last query: dict(dfd, vefd, search, calls, launches)."""
+        out = (ctypes.c_double * 7)()
+        _check(lib().rfd_context_phase_times(self._h, int(enable), out))
+        return dict(zip(("dfd_ms", "vefd_ms", "search_ms", "calls", "launches", "h2d_bytes",
+                         "d2h_bytes"), list(out)))
+
+    def fp64_peak(self):
+        """Measured FP64 FMA throughput in TFLOP/s."""
+        out = ctypes.c_double()
+        _check(lib().rfd_fp64_peak(self._h, ctypes.byref(out)))
+        return out.value
+
+    def distance_device(self, p_ptr, n1, q_ptr, n2, dims, **kw):
+        """Single pair whose curves already live in device memory (raw pointers)."""
+        o = options(memory=RFD_MEM_DEVICE, **kw)
+        r = Result()
+        _check(lib().rfd_distance(self._h, ctypes.c_void_p(p_ptr), int(n1), ctypes.c_void_p(q_ptr),
+                                  int(n2), int(dims), ctypes.byref(o), ctypes.byref(r)))
+        return r.as_dict()
+
+    # ---- single pair
+    def distance(self, P, Q, **kw):
+        P, Q = _curve(P), _curve(Q)
+        if P.shape[1] != Q.shape[1]:
+            raise ValueError("curves differ in dimension")
+        o = options(**kw)
+        r = Result()
+        _check(lib().rfd_distance(self._h, P.ctypes.data, len(P), Q.ctypes.data, len(Q), P.shape[1],
+                                  ctypes.byref(o), ctypes.byref(r)))
+        return r.as_dict()
+
+    def bounds(self, P, Q, quirks=True, dense=False):
+        P, Q = _curve(P), _curve(Q)
+        dfd = ctypes.c_double()
+        vefd = ctypes.c_double(_endpoint_host(P, Q))
+        _check(lib().rfd_bounds(self._h, P.ctypes.data, len(P), Q.ctypes.data, len(Q), P.shape[1],
+                                int(bool(quirks)), int(bool(dense)), ctypes.byref(dfd),
+                                ctypes.byref(vefd)))
+        return dfd.value, vefd.value
+
+    def decide(self, P, Q, radius, dense=False):
+        P, Q = _curve(P), _curve(Q)
+        reach = ctypes.c_int32()
+        rub = ctypes.c_double()
+        _check(lib().rfd_decide(self._h, P.ctypes.data, len(P), Q.ctypes.data, len(Q), P.shape[1],
+                                float(radius), int(bool(dense)), ctypes.byref(reach),
+                                ctypes.byref(rub)))
+        return bool(reach.value), rub.value
+
+    # ---- batch
+    def distance_batch(self, Ps, Qs, brackets=None, **kw):
+        """Ps, Qs: sequences of host arrays, or (with memory=RFD_MEM_DEVICE) of
+        (device_pointer, n, dims) tuples."""
+        n = len(Ps)
+        if n != len(Qs):
+            raise ValueError("Ps and Qs differ in length")
+        o = options(**kw)
+        keep = []
+        p1 = (ctypes.c_void_p * n)()
+        p2 = (ctypes.c_void_p * n)()
+        n1 = (ctypes.c_int64 * n)()
+        n2 = (ctypes.c_int64 * n)()
+        dm = (ctypes.c_int32 * n)()
+        for k in range(n):
+            if o.memory == RFD_MEM_DEVICE:
+                (a, la, da), (b, lb_, db) = Ps[k], Qs[k]
+                p1[k], p2[k], n1[k], n2[k], dm[k] = a, b, la, lb_, da
+            else:
+                A, B = _curve(Ps[k]), _curve(Qs[k])
+                keep += [A, B]
+                p1[k], p2[k], n1[k], n2[k], dm[k] = A.ctypes.data, B.ctypes.data, len(A), len(B), A.shape[1]
+        if brackets is not None:
+            br = np.ascontiguousarray(brackets, dtype=np.float64).reshape(n, 2)
+            keep.append(br)
+            o.bracket = br.ctypes.data_as(_dp)
+        res = (Result * n)()
+        _check(lib().rfd_distance_batch(self._h, n, p1, n1, p2, n2, dm, ctypes.byref(o), res))
+        return [r.as_dict() for r in res]
+
+
+def _endpoint_host(P, Q):
+    a = float(np.sum((P[0] - Q[0]) ** 2))
+    b = float(np.sum((P[-1] - Q[-1]) ** 2))
+    return float(np.sqrt(max(a, b)))
+
+
+_DEFAULT_CTX = None
+
+
+def default_context():
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+def compute_distance_parallel(curve1, curve2, force_oversize=False):
+    """Mirror of the reference's compute_distance_parallel (include/wrapper.hpp:4): stop rule
+    ub - lb <= FLT_EPSILON, VE-FD launch rule of the reference, result (lb + ub) / 2."""
+    del force_oversize  # accepted for compatibility; the fused O(n+m) decision always runs
+    return default_context().distance(curve1, curve2)["distance"]
+
+
+def _load(path, dims, start, limit):
+    out = _dp()
+    n = ctypes.c_int64()
+    _check(lib().rfd_load_txt(str(path).encode(), dims, int(start), int(limit), ctypes.byref(out),
+                              ctypes.byref(n)))
+    try:
+        arr = np.ctypeslib.as_array(out, shape=(n.value * dims,)).copy() if n.value else np.zeros(0)
+    finally:
+        lib().rfd_free(out)
+    return arr.reshape(n.value, dims)
+
+
+def txt_loader2(path, start=0, limit=10000000):
+    """txtLoader2 (include/txtReader.hpp:6 of the reference) as an (n, 2) array."""
+    return _load(path, 2, start, limit)
+
+
+def txt_loader3(path, start=0, limit=10000000):
+    """txtLoader3 (include/txtReader.hpp:48 of the reference) as an (n, 3) array."""
+    return _load(path, 3, start, limit)
+
+
+# ---- synthetic workloads
+def gen_pair(style, dims, n1, n2, scale, noise, seed, stream=0):
+    P = np.empty((n1, dims))
+    Q = np.empty((n2, dims))
+    m1, m2 = ctypes.c_int64(), ctypes.c_int64()
+    _check(lib().rfd_gen_pair(style, dims, n1, n2, scale, noise, seed, stream,
+                              P.ctypes.data_as(_dp), ctypes.byref(m1), Q.ctypes.data_as(_dp),
+                              ctypes.byref(m2)))
+    return P[: m1.value].copy(), Q[: m2.value].copy()
+
+
+def gen_batch_spec(config, npairs, seed):
+    dims = np.empty(npairs, np.int32)
+    n1 = np.empty(npairs, np.int64)
+    n2 = np.empty(npairs, np.int64)
+    styles = np.empty(npairs, np.int32)
+    scales = np.empty(npairs)
+    noises = np.empty(npairs)
+    _check(lib().rfd_gen_batch_spec(config, npairs, seed, dims.ctypes.data_as(_i32p),
+                                    n1.ctypes.data_as(_i64p), n2.ctypes.data_as(_i64p),
+                                    styles.ctypes.data_as(_i32p), scales.ctypes.data_as(_dp),
+                                    noises.ctypes.data_as(_dp)))
+    return dims, n1, n2, styles, scales, noises
+
+
+def gen_config(config, npairs=None, seed=None):
+    """Pairs of a benchmark workload: 0 walk 2000x1900 2D (seed 0), 1 spline 200k x 200k 3D
+    (seed 1), 2 4096 uneven pairs (seed 2), 3 training pairs (seed 3), 4 512 large 3D pairs
+    (seed 5).  Returns a list of (P, Q)."""
+    defaults = {0: (1, 0), 1: (1, 1), 2: (4096, 2), 3: (200000, 3), 4: (512, 5)}
+    dn, ds = defaults[config]
+    npairs = dn if npairs is None else npairs
+    seed = ds if seed is None else seed
+    dims, n1, n2, styles, scales, noises = gen_batch_spec(config, npairs, seed)
+    return [gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]), float(scales[k]),
+                     float(noises[k]), seed, k) for k in range(npairs)]
+
+
+def search_step(state, istate, stop_mode, have_outcome, eps, reachable):
+    """Host copy of the device search state machine (for tests)."""
+    st = (ctypes.c_double * 6)(*state)
+    ist = (ctypes.c_int32 * 4)(*istate)
+    nxt = ctypes.c_double()
+    more = lib().rfd_search_step(st, ist, stop_mode, int(bool(have_outcome)), float(eps),
+                                 int(bool(reachable)), ctypes.byref(nxt))
+    return bool(more), nxt.value, list(st), list(ist)

@@ -1,0 +1,805 @@
+// Host orchestration and C ABI of the wavefront engine (librfd.so).
+//
+// One call solves a batch of pairs (a single pair is a batch of one) with a fixed launch
+// sequence on one stream and no host synchronisation until the results are read:
+//   prep  : per-segment constants, endpoint bound, state init
+//   DFD   : dense min-max DP over the n1 x n2 points            -> ub (reference .cu:1268-1326)
+//   VE-FD : min-max DP over the (n1-1) x (n2-1) cells, pruned
+//           by DFD^2 (exact, see rfd_device.cuh)               -> lb (reference .cu:1328-1391)
+//   VE-FD : dense recomputation for pairs whose pruned pass did not reach the last cell
+//   probe : one reachability decision per active pair per launch; the warp that completes a
+//           pair's probe applies the outcome and proposes the next radius on the device
+//           (reference host loop src/frechet.cpp:36-63)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rfd.h"
+#include "rfd_device.cuh"
+
+using namespace rfd;
+
+namespace {
+
+constexpr int kBlock = 128;
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define RFD_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? RFD_ERR_NOMEM : RFD_ERR_CUDA,         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs);
+__device__ __forceinline__ void next_probe(PairState* st, int* active_pairs);
+
+__device__ __forceinline__ void finish_pair(PairState* st, int* active_pairs) {
+  st->phase = PH_DONE;
+  st->active = 0;
+  st->distance = (st->srch.ub + st->srch.lb) / 2.0;
+  atomicSub(active_pairs, 1);
+}
+
+__device__ __forceinline__ void next_probe(PairState* st, int* active_pairs) {
+  double eps;
+  if (search_next(st->srch, &eps)) {
+    st->phase = PH_SEARCH;
+    st->split = eps;
+    st->r2 = __dmul_rn(eps, eps);  // radius * radius (host product in the reference, .cu:1440)
+  } else {
+    finish_pair(st, active_pairs);
+  }
+}
+
+__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs) {
+  if (st->vefd > st->dfd) st->flags |= RFD_FLAG_LB_GT_UB;
+  search_begin(st->srch, st->vefd, st->dfd, st->blo, st->bhi);
+  next_probe(st, active_pairs);
+}
+
+template <int KIND>
+__device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
+  const double r = *(volatile double*)&st->result;
+  if (KIND == K_DFD) {
+    st->dfd = __dsqrt_rn(r);  // reference .cu:633
+    if (pd.n1 < 2 || pd.n2 < 2) {
+      // one-point curve: every coupling maps the other curve onto that point
+      st->vefd = st->dfd;
+      st->srch.lb = st->srch.ub = st->dfd;
+      st->flags |= RFD_FLAG_DEGENERATE;
+      finish_pair(st, active_pairs);
+    } else {
+      const int prod = (int)((unsigned)pd.n1 * (unsigned)pd.n2);  // int product, .cu:1343
+      if (st->quirks && prod <= 10000) {
+        st->vefd = st->endpoint;
+        st->flags |= RFD_FLAG_VEFD_SKIPPED;
+        begin_search(st, active_pairs);
+      } else {
+        st->phase = PH_VEFD;
+        // VE-FD <= CFD <= DFD; the margin absorbs rounding when they coincide.
+        st->U = st->dense ? (double)INFINITY : __dmul_rn(r, 1.0 + 0x1p-30);
+      }
+    }
+  } else if (KIND == K_VEFD) {
+    if (!(r <= st->U)) {
+      st->phase = PH_VEFD_DENSE;
+      st->U = (double)INFINITY;
+      st->flags |= RFD_FLAG_VEFD_DENSE;
+    } else {
+      st->vefd = __dsqrt_rn(r);  // reference .cu:427
+      begin_search(st, active_pairs);
+    }
+  } else {
+    st->cells_nominal += (unsigned long long)(pd.n1 - 1) * (unsigned long long)(pd.n2 - 1);
+    st->result = r;
+    if (st->decide_only) {
+      st->srch.probes += 1;
+      st->phase = PH_DONE;
+      st->active = 0;
+      atomicSub(active_pairs, 1);
+    } else {
+      search_update(st->srch, st->split, r == 1.0);  // reference .cu:1592, frechet.cpp:80-85
+      next_probe(st, active_pairs);
+    }
+  }
+  st->epoch += 1;
+  st->done_count = 0;
+  st->dead_from = INT_MAX;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
+  const int lane = threadIdx.x & 31;
+  if (bcast(lane == 0 ? ld_volatile(wa.active_pairs) : 0) == 0) return;
+  for (;;) {
+    unsigned t = 0;
+    int err = 0;
+    if (lane == 0) {
+      t = atomicAdd(wa.ticket, 1u);
+      err = ld_volatile(wa.error);
+    }
+    t = bcast(t);
+    if ((int)t >= wa.nitems || bcast(err)) return;
+    const int2 it = wa.items[t];
+    PairState* st = wa.st + it.x;
+    const int ok = lane == 0 ? (ld_volatile(&st->phase) == wa.phase && ld_volatile(&st->active)) : 0;
+    if (!bcast(ok)) continue;
+    const PairDesc pd = wa.pairs[it.x];
+    const int R = KIND == K_DFD ? pd.n1 : pd.n1 - 1;
+    const int S = (R + 31) >> 5;
+    if (it.y >= S) continue;
+    const StripOut so =
+        pd.d == 2 ? run_strip<KIND, 2>(wa, pd, st, it.y) : run_strip<KIND, 3>(wa, pd, st, it.y);
+    if (so.status) return;
+    __syncwarp();
+    if (lane == 0) {
+      if (KIND == K_DEC && so.evaluated) atomicAdd(&st->cells_eval, so.evaluated);
+      if (KIND == K_VEFD && so.evaluated) atomicAdd(&st->cells_vefd, so.evaluated);
+      __threadfence();
+      const int n = atomicAdd(&st->done_count, 1);
+      if (n == S - 1) {
+        __threadfence();
+        finalize<KIND>(st, pd, wa.active_pairs);
+        __threadfence();
+      }
+    }
+  }
+}
+
+// Per-pair constants and state.  One block per pair (grid-stride).
+__global__ void prep_kernel(const PairDesc* pairs, PairState* st, int npairs, int start_phase) {
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const PairDesc pd = pairs[p];
+    const int d = pd.d;
+    double2* rowc = const_cast<double2*>(pd.rowc);
+    double2* colrec = const_cast<double2*>(pd.colrec);
+    for (int i = threadIdx.x; i < pd.n1 - 1; i += blockDim.x) {
+      double A = 0.0;
+      for (int k = 0; k < d; ++k) {
+        const double t = __dsub_rn(pd.P[(size_t)(i + 1) * d + k], pd.P[(size_t)i * d + k]);
+        A = __fma_rn(t, t, A);
+      }
+      rowc[i] = make_double2(A, __ddiv_rn(0.5, A));
+    }
+    for (int j = threadIdx.x; j < pd.n2 - 1; j += blockDim.x) {
+      double A = 0.0;
+      double q0[3] = {0, 0, 0}, q1[3] = {0, 0, 0};
+      for (int k = 0; k < d; ++k) {
+        q0[k] = pd.Q[(size_t)j * d + k];
+        q1[k] = pd.Q[(size_t)(j + 1) * d + k];
+        const double t = __dsub_rn(q0[k], q1[k]);  // reference stages q_j - q_{j+1} (.cu:1137)
+        A = __fma_rn(t, t, A);
+      }
+      const double inv = __ddiv_rn(0.5, A);
+      if (d == 2) {
+        double2* r = colrec + (size_t)j * 3;
+        r[0] = make_double2(q0[0], q0[1]);
+        r[1] = make_double2(q1[0], q1[1]);
+        r[2] = make_double2(A, inv);
+      } else {
+        double2* r = colrec + (size_t)j * 4;
+        r[0] = make_double2(q0[0], q0[1]);
+        r[1] = make_double2(q0[2], q1[0]);
+        r[2] = make_double2(q1[1], q1[2]);
+        r[3] = make_double2(A, inv);
+      }
+    }
+    if (threadIdx.x == 0) {
+      PairState* s = st + p;
+      // endpoint bound: host arithmetic in the reference, no fusion (src/frechet.cpp:30)
+      double a = 0.0, b = 0.0;
+      for (int k = 0; k < d; ++k) {
+        const double t0 = __dsub_rn(pd.P[k], pd.Q[k]);
+        a = __dadd_rn(a, __dmul_rn(t0, t0));
+        const double t1 = __dsub_rn(pd.P[(size_t)(pd.n1 - 1) * d + k], pd.Q[(size_t)(pd.n2 - 1) * d + k]);
+        b = __dadd_rn(b, __dmul_rn(t1, t1));
+      }
+      s->endpoint = __dsqrt_rn(a < b ? b : a);
+      s->seed = __dmul_rn(s->endpoint, s->endpoint);  // init_value * init_value, .cu:259
+      s->epoch = 1;
+      s->done_count = 0;
+      s->dead_from = INT_MAX;
+      s->U = (double)INFINITY;
+      s->active = 1;
+      s->phase = start_phase;
+    }
+  }
+}
+
+// FP64 FMA throughput probe: 8 independent chains per thread, values kept finite.
+__global__ void __launch_bounds__(256) fp64_fma_kernel(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = __fma_rn(x[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1234.5) out[0] = s;  // keeps the chains live without a store per thread
+}
+
+}  // namespace
+
+// ============================================================================ context
+
+struct rfd_context {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int grid[3] = {0, 0, 0};
+  void* dws = nullptr;
+  size_t dws_size = 0;
+  void* hws = nullptr;
+  size_t hws_size = 0;
+  long long spin_cycles = 0;
+  // phase timing (rfd_context_phase_times)
+  int timing = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace {
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int ensure_device(rfd_context* ctx, size_t bytes) {
+  if (bytes <= ctx->dws_size) return RFD_OK;
+  if (ctx->dws) cudaFree(ctx->dws);
+  ctx->dws = nullptr;
+  ctx->dws_size = 0;
+  size_t want = std::max(bytes, ctx->dws_size + ctx->dws_size / 4);
+  cudaError_t e = cudaMalloc(&ctx->dws, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMalloc(&ctx->dws, bytes);
+    want = bytes;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RFD_ERR_NOMEM, "device workspace of " + std::to_string(bytes) + " bytes");
+  }
+  ctx->dws_size = want;
+  return RFD_OK;
+}
+
+int ensure_host(rfd_context* ctx, size_t bytes) {
+  if (bytes <= ctx->hws_size) return RFD_OK;
+  if (ctx->hws) cudaFreeHost(ctx->hws);
+  ctx->hws = nullptr;
+  ctx->hws_size = 0;
+  size_t want = std::max(bytes, ctx->hws_size + ctx->hws_size / 4);
+  if (cudaMallocHost(&ctx->hws, want) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RFD_ERR_NOMEM, "pinned staging of " + std::to_string(want) + " bytes");
+  }
+  ctx->hws_size = want;
+  return RFD_OK;
+}
+
+enum Mode { MODE_DISTANCE = 0, MODE_BOUNDS = 1, MODE_DECIDE = 2 };
+
+struct Layout {
+  // device offsets
+  size_t descs, states, items, counters, error, active, zero_begin, zero_end, total;
+  std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog;
+  // host staging offsets
+  size_t h_descs, h_states, h_items, h_misc, h_curves, h_total;
+  std::vector<size_t> hP, hQ;
+  int nitems, nlaunch;
+};
+
+int check_pair(const double* c1, int64_t n1, const double* c2, int64_t n2, int32_t d) {
+  if (!c1 || !c2) return fail(RFD_ERR_ARG, "null curve pointer");
+  if (d != 2 && d != 3) return fail(RFD_ERR_ARG, "dims must be 2 or 3");
+  if (n1 < 1 || n2 < 1) return fail(RFD_ERR_ARG, "empty curve");
+  if (n1 > (1 << 30) || n2 > (1 << 30)) return fail(RFD_ERR_LIMIT, "curve longer than 2^30 points");
+  return RFD_OK;
+}
+
+int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
+              const double* const* c2s, const int64_t* n2s, const int32_t* dims,
+              const rfd_options* opt, rfd_result* out, int mode, double radius) {
+  if (!ctx || npairs < 0 || (npairs > 0 && (!c1s || !n1s || !c2s || !n2s || !dims || !out)))
+    return fail(RFD_ERR_ARG, "null argument");
+  if (npairs == 0) return RFD_OK;
+  if (npairs > (1 << 24)) return fail(RFD_ERR_LIMIT, "more than 2^24 pairs");
+  rfd_options o;
+  rfd_options_init(&o, 0);
+  if (opt) o = *opt;
+  if (o.max_probes < 0 || o.max_probes > RFD_MAX_PROBES) return fail(RFD_ERR_ARG, "max_probes");
+  if (o.stop_mode != RFD_STOP_ABS && o.stop_mode != RFD_STOP_REL) return fail(RFD_ERR_ARG, "stop_mode");
+  if (!(o.tol >= 0.0)) return fail(RFD_ERR_ARG, "tol");
+  for (int64_t p = 0; p < npairs; ++p) {
+    int rc = check_pair(c1s[p], n1s[p], c2s[p], n2s[p], dims[p]);
+    if (rc) return rc;
+    if (mode != MODE_DISTANCE && (n1s[p] < 2 || n2s[p] < 2))
+      return fail(RFD_ERR_ARG, "bounds and decisions need curves of at least two points");
+  }
+  const bool on_device = o.memory == RFD_MEM_DEVICE;
+  const int max_probes = mode == MODE_DISTANCE ? o.max_probes : 0;
+
+  // ---------------- layout
+  Layout L;
+  L.P.resize(npairs); L.Q.resize(npairs); L.rowc.resize(npairs); L.colrec.resize(npairs);
+  L.bnd.resize(npairs); L.tags.resize(npairs); L.prog.resize(npairs);
+  L.hP.resize(npairs); L.hQ.resize(npairs);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t r = off; off = align_up(off + bytes, 256); return r; };
+  L.descs = take(sizeof(PairDesc) * npairs);
+  L.states = take(sizeof(PairState) * npairs);
+  // items: interleave pairs by strip index so early strips of every pair go first
+  std::vector<int> order(npairs);
+  for (int64_t p = 0; p < npairs; ++p) order[p] = (int)p;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (double)n1s[a] * (double)n2s[a] > (double)n1s[b] * (double)n2s[b];
+  });
+  int64_t maxS = 0, nitems = 0;
+  for (int64_t p = 0; p < npairs; ++p) {
+    int64_t S = (n1s[p] + 31) / 32;
+    maxS = std::max(maxS, S);
+    nitems += S;
+  }
+  if (nitems > INT32_MAX / 2) return fail(RFD_ERR_LIMIT, "too many strips");
+  L.nitems = (int)nitems;
+  L.items = take(sizeof(int2) * nitems);
+  L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0);
+  L.zero_begin = off;
+  L.counters = take(sizeof(unsigned) * L.nlaunch);
+  L.error = take(sizeof(int));
+  for (int64_t p = 0; p < npairs; ++p) {
+    const int64_t n1 = n1s[p], n2 = n2s[p];
+    const int64_t S = (n1 + 31) / 32;
+    const int64_t cstride = align_up((size_t)n2, 32);
+    const int64_t tstride = align_up((size_t)((n2 + 31) / 32), 32);
+    L.tags[p] = take(sizeof(unsigned) * (S > 1 ? S - 1 : 0) * tstride);
+    L.prog[p] = take(sizeof(Prog) * S);
+  }
+  L.zero_end = off;
+  L.active = take(sizeof(int));
+  for (int64_t p = 0; p < npairs; ++p) {
+    const int64_t n1 = n1s[p], n2 = n2s[p];
+    const int d = dims[p];
+    const int64_t S = (n1 + 31) / 32;
+    const int64_t cstride = align_up((size_t)n2, 32);
+    if (!on_device) {
+      L.P[p] = take(sizeof(double) * n1 * d);
+      L.Q[p] = take(sizeof(double) * n2 * d);
+    }
+    L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(n1 - 1, 1));
+    L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(n2 - 1, 1));
+    L.bnd[p] = take(sizeof(double) * (S > 1 ? S - 1 : 0) * cstride);
+  }
+  L.total = off;
+
+  size_t hoff = 0;
+  auto htake = [&](size_t bytes) { size_t r = hoff; hoff = align_up(hoff + bytes, 256); return r; };
+  L.h_descs = htake(sizeof(PairDesc) * npairs);
+  L.h_states = htake(sizeof(PairState) * npairs);
+  L.h_items = htake(sizeof(int2) * nitems);
+  L.h_misc = htake(4 * sizeof(int));
+  L.h_curves = hoff;
+  if (!on_device) {
+    for (int64_t p = 0; p < npairs; ++p) {
+      L.hP[p] = htake(sizeof(double) * n1s[p] * dims[p]);
+      L.hQ[p] = htake(sizeof(double) * n2s[p] * dims[p]);
+    }
+  }
+  L.h_total = hoff;
+
+  int rc = ensure_device(ctx, L.total);
+  if (rc) return rc;
+  rc = ensure_host(ctx, L.h_total);
+  if (rc) return rc;
+  char* dbase = (char*)ctx->dws;
+  char* hbase = (char*)ctx->hws;
+
+  // ---------------- host staging
+  PairDesc* hd = (PairDesc*)(hbase + L.h_descs);
+  PairState* hs = (PairState*)(hbase + L.h_states);
+  int2* hi = (int2*)(hbase + L.h_items);
+  for (int64_t p = 0; p < npairs; ++p) {
+    const int64_t n1 = n1s[p], n2 = n2s[p];
+    const int d = dims[p];
+    const int64_t S = (n1 + 31) / 32;
+    PairDesc& D = hd[p];
+    memset(&D, 0, sizeof(D));
+    if (on_device) {
+      D.P = c1s[p];
+      D.Q = c2s[p];
+    } else {
+      memcpy(hbase + L.hP[p], c1s[p], sizeof(double) * n1 * d);
+      memcpy(hbase + L.hQ[p], c2s[p], sizeof(double) * n2 * d);
+      D.P = (const double*)(dbase + L.P[p]);
+      D.Q = (const double*)(dbase + L.Q[p]);
+    }
+    D.rowc = (const double2*)(dbase + L.rowc[p]);
+    D.colrec = (const double2*)(dbase + L.colrec[p]);
+    D.bnd = (double*)(dbase + L.bnd[p]);
+    D.tags = (unsigned*)(dbase + L.tags[p]);
+    D.prog = (Prog*)(dbase + L.prog[p]);
+    D.n1 = (int)n1;
+    D.n2 = (int)n2;
+    D.d = d;
+    D.cstride = (long long)align_up((size_t)n2, 32);
+    D.tstride = (long long)align_up((size_t)((n2 + 31) / 32), 32);
+    (void)S;
+    PairState& s = hs[p];
+    memset(&s, 0, sizeof(s));
+    s.srch.tol = o.tol;
+    s.srch.stop_mode = o.stop_mode;
+    s.srch.max_probes = max_probes;
+    s.quirks = o.reference_quirks;
+    s.dense = o.dense;
+    s.blo = s.bhi = NAN;
+    if (o.bracket && mode == MODE_DISTANCE) {
+      s.blo = o.bracket[2 * p];
+      s.bhi = o.bracket[2 * p + 1];
+    }
+    if (mode == MODE_DECIDE) {
+      s.decide_only = 1;
+      s.split = radius;
+      s.r2 = radius * radius;
+    }
+  }
+  {
+    int64_t k = 0;
+    for (int64_t sidx = 0; sidx < maxS; ++sidx)
+      for (int64_t q = 0; q < npairs; ++q) {
+        const int p = order[q];
+        if (sidx < (n1s[p] + 31) / 32) hi[k++] = make_int2(p, (int)sidx);
+      }
+  }
+
+  // ---------------- transfers
+  cudaStream_t st = ctx->stream;
+  size_t h2d_bytes = sizeof(PairDesc) * npairs + sizeof(PairState) * npairs + sizeof(int2) * nitems +
+                     sizeof(int);
+  if (!on_device)
+    for (int64_t p = 0; p < npairs; ++p) h2d_bytes += sizeof(double) * (n1s[p] + n2s[p]) * dims[p];
+  RFD_CUDA(cudaMemcpyAsync(dbase + L.descs, hbase + L.h_descs, sizeof(PairDesc) * npairs,
+                           cudaMemcpyHostToDevice, st));
+  RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * npairs,
+                           cudaMemcpyHostToDevice, st));
+  RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
+                           cudaMemcpyHostToDevice, st));
+  if (!on_device) {
+    // curves are staged contiguously; one copy per pair keeps device offsets independent
+    for (int64_t p = 0; p < npairs; ++p) {
+      RFD_CUDA(cudaMemcpyAsync(dbase + L.P[p], hbase + L.hP[p], sizeof(double) * n1s[p] * dims[p],
+                               cudaMemcpyHostToDevice, st));
+      RFD_CUDA(cudaMemcpyAsync(dbase + L.Q[p], hbase + L.hQ[p], sizeof(double) * n2s[p] * dims[p],
+                               cudaMemcpyHostToDevice, st));
+    }
+  }
+  RFD_CUDA(cudaMemsetAsync(dbase + L.zero_begin, 0, L.zero_end - L.zero_begin, st));
+  int* hmisc = (int*)(hbase + L.h_misc);  // [0] active pairs, [1] error word read back
+  hmisc[0] = (int)npairs;
+  hmisc[1] = 0;
+  RFD_CUDA(cudaMemcpyAsync(dbase + L.active, hmisc, sizeof(int), cudaMemcpyHostToDevice, st));
+
+  // ---------------- launches
+  const PairDesc* dd = (const PairDesc*)(dbase + L.descs);
+  PairState* ds = (PairState*)(dbase + L.states);
+  const int start_phase = mode == MODE_DECIDE ? PH_SEARCH : PH_DFD;
+  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[0], st));
+  int launches = 1;
+  prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dd, ds, (int)npairs,
+                                                                                start_phase);
+  RFD_CUDA(cudaGetLastError());
+  WaveArgs wa;
+  wa.pairs = dd;
+  wa.st = ds;
+  wa.items = (const int2*)(dbase + L.items);
+  wa.nitems = L.nitems;
+  wa.error = (int*)(dbase + L.error);
+  wa.active_pairs = (int*)(dbase + L.active);
+  wa.spin_cycles = ctx->spin_cycles;
+  unsigned* counters = (unsigned*)(dbase + L.counters);
+  int li = 0;
+  if (mode != MODE_DECIDE) {
+    wa.phase = PH_DFD;
+    wa.ticket = counters + li++;
+    wave_kernel<K_DFD><<<ctx->grid[K_DFD], kBlock, 0, st>>>(wa);
+    RFD_CUDA(cudaGetLastError());
+    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
+    wa.phase = PH_VEFD;
+    wa.ticket = counters + li++;
+    wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
+    RFD_CUDA(cudaGetLastError());
+    wa.phase = PH_VEFD_DENSE;
+    wa.ticket = counters + li++;
+    wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
+    RFD_CUDA(cudaGetLastError());
+    launches += 3;
+  }
+  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
+  const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
+  for (int k = 0; k < nprobe; ++k) {
+    wa.phase = PH_SEARCH;
+    wa.ticket = counters + li++;
+    wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
+    RFD_CUDA(cudaGetLastError());
+    ++launches;
+  }
+  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[3], st));
+
+  // ---------------- results
+  RFD_CUDA(cudaMemcpyAsync(hs, ds, sizeof(PairState) * npairs, cudaMemcpyDeviceToHost, st));
+  RFD_CUDA(cudaMemcpyAsync(hmisc + 1, wa.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  RFD_CUDA(cudaStreamSynchronize(st));
+  if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
+  if (ctx->timing) {
+    float a = 0.f, b = 0.f, c = 0.f;
+    if (mode != MODE_DECIDE) {
+      RFD_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+      RFD_CUDA(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
+      RFD_CUDA(cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]));
+    } else {
+      RFD_CUDA(cudaEventElapsedTime(&c, ctx->ev[0], ctx->ev[3]));
+    }
+    ctx->acc[0] += a;
+    ctx->acc[1] += b;
+    ctx->acc[2] += c;
+    ctx->acc[3] += 1;
+    ctx->acc[4] += launches;
+  }
+  ctx->acc[5] += (double)h2d_bytes;
+  ctx->acc[6] += (double)(sizeof(PairState) * npairs + sizeof(int));
+  for (int64_t p = 0; p < npairs; ++p) {
+    const PairState& s = hs[p];
+    rfd_result& r = out[p];
+    memset(&r, 0, sizeof(r));
+    r.dfd = s.dfd;
+    r.vefd = s.vefd;
+    r.endpoint = s.endpoint;
+    r.lb = s.srch.lb;
+    r.ub = s.srch.ub;
+    r.distance = s.distance;
+    r.probes = s.srch.probes;
+    r.flags = s.flags | s.srch.flags;
+    r.cells_nominal = (int64_t)s.cells_nominal;
+    r.cells_evaluated = (int64_t)s.cells_eval;
+    r.cells_fp64 = (int64_t)s.cells_eval;
+    r.cells_vefd = (int64_t)s.cells_vefd;
+    if (mode == MODE_DECIDE) r.distance = s.result;  // propagated right UB of the last cell
+    if (mode == MODE_DISTANCE && s.phase != PH_DONE)
+      return fail(RFD_ERR_INTERNAL, "pair " + std::to_string(p) + " did not finish");
+  }
+  return RFD_OK;
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+
+extern "C" {
+
+int32_t rfd_abi_version(void) { return RFD_ABI_VERSION; }
+
+const char* rfd_status_string(int32_t s) {
+  switch (s) {
+    case RFD_OK: return "ok";
+    case RFD_ERR_ARG: return "invalid argument";
+    case RFD_ERR_CUDA: return "CUDA error";
+    case RFD_ERR_NOMEM: return "out of memory";
+    case RFD_ERR_TIMEOUT: return "inter-warp wait timed out";
+    case RFD_ERR_NODEV: return "no CUDA device";
+    case RFD_ERR_INTERNAL: return "internal error";
+    case RFD_ERR_LIMIT: return "size limit exceeded";
+    default: return "unknown status";
+  }
+}
+
+const char* rfd_last_error(void) { return g_last_error.c_str(); }
+
+void rfd_options_init(rfd_options* o, int32_t precise) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  if (precise) {
+    o->stop_mode = RFD_STOP_REL;
+    o->tol = 0x1p-33;
+    o->reference_quirks = 0;
+  } else {
+    o->stop_mode = RFD_STOP_ABS;
+    o->tol = (double)FLT_EPSILON;
+    o->reference_quirks = 1;
+  }
+  o->max_probes = 64;
+  o->dense = 0;
+  o->precision = RFD_PREC_FP64;
+  o->memory = RFD_MEM_HOST;
+  o->bracket = nullptr;
+}
+
+int32_t rfd_context_create(int32_t device, rfd_context** out) {
+  if (!out) return fail(RFD_ERR_ARG, "null context pointer");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(RFD_ERR_NODEV, "no CUDA device");
+  }
+  if (device < 0 || device >= n) return fail(RFD_ERR_ARG, "device index");
+  RFD_CUDA(cudaSetDevice(device));
+  rfd_context* c = new rfd_context();
+  c->device = device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    delete c;
+    return fail(RFD_ERR_CUDA, "cudaGetDeviceProperties");
+  }
+  c->num_sms = prop.multiProcessorCount;
+  int occ[3] = {0, 0, 0};
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], wave_kernel<K_DFD>, kBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], wave_kernel<K_VEFD>, kBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], wave_kernel<K_DEC>, kBlock, 0);
+  for (int k = 0; k < 3; ++k) c->grid[k] = std::max(1, occ[k]) * c->num_sms;
+  // wait budget: about 20 s at the maximum SM clock
+  c->spin_cycles = (long long)prop.clockRate * 1000LL * 20LL;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(RFD_ERR_CUDA, "cudaStreamCreate");
+  }
+  c->stream = c->own_stream;
+  *out = c;
+  return RFD_OK;
+}
+
+int32_t rfd_context_destroy(rfd_context* ctx) {
+  if (!ctx) return RFD_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->dws) cudaFree(ctx->dws);
+  if (ctx->hws) cudaFreeHost(ctx->hws);
+  for (int k = 0; k < 4; ++k)
+    if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return RFD_OK;
+}
+
+int32_t rfd_context_phase_times(rfd_context* ctx, int32_t enable, double* out) {
+  if (!ctx) return fail(RFD_ERR_ARG, "null context");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  if (enable > 0 && !ctx->ev[0])
+    for (int k = 0; k < 4; ++k) RFD_CUDA(cudaEventCreate(&ctx->ev[k]));
+  if (enable >= 0) ctx->timing = enable > 0;
+  if (out) {
+    for (int k = 0; k < 7; ++k) {
+      out[k] = ctx->acc[k];
+      ctx->acc[k] = 0;
+    }
+  }
+  return RFD_OK;
+}
+
+int32_t rfd_fp64_peak(rfd_context* ctx, double* tflops) {
+  if (!ctx || !tflops) return fail(RFD_ERR_ARG, "null argument");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  int per_sm = 0;
+  RFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fp64_fma_kernel, 256, 0));
+  const int blocks = std::max(1, per_sm) * ctx->num_sms;
+  const int iters = 1 << 14;
+  double* scratch = nullptr;
+  RFD_CUDA(cudaMalloc(&scratch, sizeof(double)));
+  cudaEvent_t e0, e1;
+  RFD_CUDA(cudaEventCreate(&e0));
+  RFD_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(e0, ctx->stream);
+    fp64_fma_kernel<<<blocks, 256, 0, ctx->stream>>>(scratch, iters, 0.999999, 1e-7);
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return fail(RFD_ERR_CUDA, cudaGetErrorString(e));
+  const double flops = 2.0 * 8.0 * (double)iters * (double)blocks * 256.0;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return RFD_OK;
+}
+
+int32_t rfd_context_set_stream(rfd_context* ctx, void* stream) {
+  if (!ctx) return fail(RFD_ERR_ARG, "null context");
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return RFD_OK;
+}
+
+int32_t rfd_distance(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                     int32_t dims, const rfd_options* opt, rfd_result* out) {
+  if (!ctx) return fail(RFD_ERR_ARG, "null context");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  return run_batch(ctx, 1, &c1, &n1, &c2, &n2, &dims, opt, out, MODE_DISTANCE, 0.0);
+}
+
+int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s,
+                           const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
+                           const int32_t* dims, const rfd_options* opt, rfd_result* out) {
+  if (!ctx) return fail(RFD_ERR_ARG, "null context");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+}
+
+int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                   int32_t dims, int32_t reference_quirks, int32_t dense, double* dfd, double* vefd) {
+  if (!ctx || !dfd || !vefd) return fail(RFD_ERR_ARG, "null argument");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  rfd_options o;
+  rfd_options_init(&o, 0);
+  o.reference_quirks = reference_quirks;
+  o.dense = dense;
+  rfd_result r;
+  int rc = run_batch(ctx, 1, &c1, &n1, &c2, &n2, &dims, &o, &r, MODE_BOUNDS, 0.0);
+  if (rc) return rc;
+  *dfd = r.dfd;
+  if (!(r.flags & RFD_FLAG_VEFD_SKIPPED)) *vefd = r.vefd;
+  return RFD_OK;
+}
+
+int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
+                   int32_t dims, double radius, int32_t dense, int32_t* reachable, double* right_ub) {
+  if (!ctx || !reachable) return fail(RFD_ERR_ARG, "null argument");
+  if (!(radius >= 0.0)) return fail(RFD_ERR_ARG, "radius");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  rfd_options o;
+  rfd_options_init(&o, 0);
+  o.dense = dense;
+  rfd_result r;
+  int rc = run_batch(ctx, 1, &c1, &n1, &c2, &n2, &dims, &o, &r, MODE_DECIDE, radius);
+  if (rc) return rc;
+  *reachable = r.distance == 1.0;
+  if (right_ub) *right_ub = r.distance;
+  return RFD_OK;
+}
+
+int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32_t have_outcome,
+                        double eps, int32_t reachable, double* next_eps) {
+  if (!state || !istate || !next_eps) return fail(RFD_ERR_ARG, "null argument");
+  Search s;
+  s.lb = state[0];
+  s.ub = state[1];
+  s.lo = state[2];
+  s.hi = state[3];
+  s.tol = state[4];
+  s.mode = istate[0];
+  s.probes = istate[1];
+  s.max_probes = istate[2];
+  s.flags = istate[3];
+  s.stop_mode = stop_mode;
+  if (have_outcome) search_update(s, eps, reachable != 0);
+  double e = 0.0;
+  const int more = search_next(s, &e) ? 1 : 0;
+  state[0] = s.lb;
+  state[1] = s.ub;
+  state[2] = s.lo;
+  state[3] = s.hi;
+  istate[0] = s.mode;
+  istate[1] = s.probes;
+  istate[3] = s.flags;
+  *next_eps = e;
+  return more;
+}
+
+}  // extern "C"

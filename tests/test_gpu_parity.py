@@ -1,0 +1,133 @@
+"""CUDA path (through the C ABI) against the CPU oracle on seeded inputs.
+
+Bar: bit-exact.  DFD and VE-FD are compared as the doubles the reference reports
+(sqrt of the DP value), every decision's propagated right UB must be identical, and a
+full search must reproduce the oracle's probe count and distance bit for bit (both run
+the same bisection on the same decisions).
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def walk_pair(seed, n1, n2, d=2, noise=0.05):
+    rng = np.random.default_rng(seed)
+    P = np.cumsum(rng.normal(size=(n1, d)), 0)
+    idx = np.linspace(0, n1 - 1, n2)
+    base = np.stack([np.interp(idx, np.arange(n1), P[:, k]) for k in range(d)], 1)
+    return P, base + rng.normal(scale=noise, size=(n2, d))
+
+
+# sizes around the 32-row strip and 32-column chunk boundaries, both orientations
+SIZES = [(2, 2), (2, 40), (40, 2), (3, 3), (31, 31), (32, 33), (33, 32), (34, 65), (65, 34),
+         (64, 64), (97, 130), (200, 150), (257, 31), (31, 257)]
+
+
+@pytest.mark.parametrize("n1,n2", SIZES)
+@pytest.mark.parametrize("d", [2, 3])
+def test_bounds_bitexact(ctx, n1, n2, d):
+    P, Q = walk_pair(n1 * 1000 + n2 + d, n1, n2, d)
+    lb = oracle.endpoint(P, Q)
+    want_dfd = np.sqrt(oracle.dfd_sq(P, Q))
+    want_vefd = np.sqrt(oracle.vefd_sq(P, Q, lb))
+    for dense in (False, True):
+        dfd, vefd = ctx.bounds(P, Q, quirks=False, dense=dense)
+        assert dfd == want_dfd, (dense, dfd, want_dfd)
+        assert vefd == want_vefd, (dense, vefd, want_vefd)
+
+
+@pytest.mark.parametrize("n1,n2", SIZES)
+@pytest.mark.parametrize("d", [2, 3])
+def test_decisions_bitexact(ctx, n1, n2, d):
+    P, Q = walk_pair(n1 * 7 + n2 * 3 + d, n1, n2, d)
+    r = oracle.distance(P, Q, stop_mode=1, quirks=False)
+    fd = r["distance"]
+    radii = [r["endpoint"], fd * 0.5, fd * (1 - 1e-6), fd, fd * (1 + 1e-6), fd * 1.5, r["dfd"],
+             r["dfd"] * 3]
+    for e in radii:
+        want_reach, want_ub = oracle.decide(P, Q, e)
+        for dense in (False, True):
+            reach, ub = ctx.decide(P, Q, e, dense=dense)
+            assert ub == want_ub and reach == want_reach, (e, dense, ub, want_ub)
+
+
+@pytest.mark.parametrize("seed,n1,n2,d", [(0, 120, 90, 2), (1, 90, 160, 3), (2, 300, 280, 2),
+                                          (3, 64, 400, 3), (4, 700, 650, 3)])
+@pytest.mark.parametrize("precise", [False, True])
+def test_distance_bitexact(ctx, seed, n1, n2, d, precise):
+    P, Q = walk_pair(seed, n1, n2, d)
+    want = oracle.distance(P, Q, stop_mode=1 if precise else 0, quirks=not precise, threads=4)
+    for dense in (False, True):
+        got = ctx.distance(P, Q, precise=precise, dense=dense)
+        assert got["probes"] == want["probes"]
+        assert got["dfd"] == want["dfd"] and got["vefd"] == want["vefd"]
+        assert got["lb"] == want["lb"] and got["ub"] == want["ub"]
+        assert got["distance"] == want["distance"]
+
+
+def test_config0_distance_bitexact(ctx, built):
+    P, Q = built.gen_config(0)[0]
+    want = oracle.distance(P, Q, stop_mode=1, quirks=False, threads=8)
+    got = ctx.distance(P, Q, precise=True)
+    assert got["distance"] == want["distance"] and got["probes"] == want["probes"]
+    ref = oracle.distance(P, Q, stop_mode=0, quirks=True, threads=8)
+    got = ctx.distance(P, Q)
+    assert got["distance"] == ref["distance"] and got["probes"] == ref["probes"]
+    assert got["cells_evaluated"] < got["cells_nominal"]
+
+
+def test_spline_pairs_bitexact(ctx, built):
+    for style, d, n1, n2 in [(1, 3, 800, 900), (1, 2, 1000, 700), (0, 3, 500, 650)]:
+        P, Q = built.gen_pair(style, d, n1, n2, 100.0 if style else 1.0, 0.1, 11, n1)
+        want = oracle.distance(P, Q, stop_mode=1, quirks=False, threads=8)
+        got = ctx.distance(P, Q, precise=True)
+        assert got["distance"] == want["distance"] and got["probes"] == want["probes"]
+
+
+def test_batch_equals_single(ctx, built):
+    pairs = [walk_pair(s, 20 + 37 * s, 15 + 53 * s, 2 + s % 2) for s in range(12)]
+    singles = [ctx.distance(P, Q, precise=True) for P, Q in pairs]
+    batch = ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True)
+    for a, b in zip(singles, batch):
+        assert a["distance"] == b["distance"] and a["probes"] == b["probes"]
+
+
+def test_degenerate_single_point(ctx):
+    P = np.array([[1.0, 2.0]])
+    Q = np.array([[0.0, 0.0], [3.0, 4.0], [1.0, 5.0]])
+    want = max(np.linalg.norm(Q - P[0], axis=1))
+    r = ctx.distance(P, Q, precise=True)
+    assert abs(r["distance"] - want) <= 1e-15 * want
+    r = ctx.distance(Q, P, precise=True)
+    assert abs(r["distance"] - want) <= 1e-15 * want
+
+
+def test_compute_distance_parallel_mirror(ctx, built):
+    P, Q = walk_pair(5, 150, 120, 2)
+    want = oracle.distance(P, Q, stop_mode=0, quirks=True)
+    assert built.compute_distance_parallel(P, Q) == want["distance"]
+
+
+@pytest.mark.parametrize("style,d,n", [(1, 3, 20000), (0, 2, 12000), (1, 2, 30000)])
+def test_sparse_equals_dense_large(ctx, built, style, d, n):
+    """Size-independent property at sizes where consumer strips outrun their producers:
+    the pruned / skipping sweeps give the dense results bit for bit, the pruned VE-FD
+    needs no dense fallback, and decisions are monotone around the result."""
+    P, Q = built.gen_pair(style, d, n, n - 1000, 100.0 if style else 1.0, 0.1, 123, n)
+    dfd_d, vefd_d = ctx.bounds(P, Q, quirks=False, dense=True)
+    dfd_s, vefd_s = ctx.bounds(P, Q, quirks=False, dense=False)
+    assert (dfd_s, vefd_s) == (dfd_d, vefd_d)
+    r = ctx.distance(P, Q, precise=True)
+    assert not (r["flags"] & built.FLAG_VEFD_DENSE)
+    assert r["vefd"] == vefd_d and r["dfd"] == dfd_d
+    assert r["vefd"] <= r["distance"] <= r["dfd"]
+    fd = r["distance"]
+    for e in (r["vefd"], fd * (1 - 1e-7), fd * (1 + 1e-7), (fd + r["dfd"]) / 2):
+        sparse = ctx.decide(P, Q, e)
+        dense = ctx.decide(P, Q, e, dense=True)
+        assert sparse == dense, (e, sparse, dense)
+    assert not ctx.decide(P, Q, fd * (1 - 1e-7))[0]
+    assert ctx.decide(P, Q, fd * (1 + 1e-7))[0]
