@@ -43,6 +43,9 @@ def lib():
         L.rfd_oracle_distance.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, _dp, _ip, _dp, _ip]
+        L.rfd_oracle_search.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_int, _dp, _ip]
         L.rfd_oracle_max_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -124,3 +127,17 @@ def distance(P, Q, stop_mode=0, tol=None, quirks=True, max_probes=200, threads=1
         "probe_eps": [log_eps[k] for k in range(n)],
         "probe_dec": [bool(log_dec[k]) for k in range(n)],
     }
+
+
+def search(P, Q, lb, ub, stop_mode=0, tol=None, max_probes=200, threads=1):
+    """Bisection from a given bracket; returns (distance, lb, ub, probes)."""
+    P, Q = _arr(P), _arr(Q)
+    if tol is None:
+        tol = FLT_EPSILON if stop_mode == 0 else REL_TOL
+    out = (ctypes.c_double * 3)()
+    probes = ctypes.c_int()
+    rc = lib().rfd_oracle_search(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], lb, ub, stop_mode,
+                                 tol, max_probes, threads, out, ctypes.byref(probes))
+    if rc:
+        raise RuntimeError(f"oracle search failed ({rc})")
+    return out[0], out[1], out[2], probes.value

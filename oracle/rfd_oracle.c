@@ -359,6 +359,31 @@ int rfd_oracle_distance(const double* P, int64_t n1, const double* Q, int64_t n2
   return 0;
 }
 
+/* Bisection from a given bracket [lb, ub] (src/frechet.cpp:36-63 with the reference's own
+   bounds), so a recorded reference search can be replayed decision by decision. */
+int rfd_oracle_search(const double* P, int64_t n1, const double* Q, int64_t n2, int d, double lb,
+                      double ub, int stop_mode, double tol, int max_probes, int threads,
+                      double* out /* [distance, lb, ub] */, int* out_probes) {
+  int probes = 0;
+  for (;;) {
+    double gap = ub - lb;
+    int open = stop_mode == 0 ? (gap > tol) : (gap > tol * ub);
+    if (!open || probes >= max_probes) break;
+    double split = (ub + lb) / 2.0;
+    if (!(split > lb && split < ub)) break;
+    double rub;
+    if (rfd_oracle_decide(P, n1, Q, n2, d, split, threads, &rub)) return -2;
+    ++probes;
+    if (rub == 1.0) ub = split;
+    else lb = split;
+  }
+  out[0] = (ub + lb) / 2.0;
+  out[1] = lb;
+  out[2] = ub;
+  *out_probes = probes;
+  return 0;
+}
+
 int rfd_oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -16,12 +16,14 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "rfd.h"
 #include "rfd_device.cuh"
+#include "rfd_team.cuh"
 
 using namespace rfd;
 
@@ -159,6 +161,78 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
   }
 }
 
+// VE-FD and decision strips with the geometry computed off the dependency chain
+// (rfd_team.cuh): one CTA per strip, warp 0 propagates, warps 1..3 fill tiles.
+template <int KIND>
+__global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
+  extern __shared__ __align__(128) unsigned char team_smem[];
+  TeamShared* sh = (TeamShared*)team_smem;
+  double2* tiles = (double2*)(team_smem + 256);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; ++k) {
+      mbar_init(&sh->full[k], 3);
+      mbar_init(&sh->req[k], 1);
+    }
+  }
+  __syncthreads();
+  unsigned seqP = 0, seqC = 0, seqH = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int go = 0, quit = 0;
+      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error)) {
+        quit = 1;
+      } else {
+        const unsigned t = atomicAdd(wa.ticket, 1u);
+        if ((int)t >= wa.nitems) {
+          quit = 1;
+        } else {
+          const int2 it = wa.items[t];
+          PairState* st = wa.st + it.x;
+          const int S = (wa.pairs[it.x].n1 - 1 + 31) >> 5;
+          if (ld_volatile(&st->phase) == wa.phase && ld_volatile(&st->active) && it.y < S) {
+            go = 1;
+            sh->item_pair = it.x;
+            sh->item_strip = it.y;
+          }
+        }
+      }
+      sh->go = go;
+      sh->quit = quit;
+      sh->evaluated = 0ull;
+      sh->status = 0;
+    }
+    __syncthreads();
+    const int go = sh->go, quit = sh->quit, p = sh->item_pair, s = sh->item_strip;
+    __syncthreads();
+    if (quit) break;
+    if (!go) continue;
+    const PairDesc pd = wa.pairs[p];
+    PairState* st = wa.st + p;
+    if (warp == 0) {
+      const int status = pd.d == 2 ? team_propagator<KIND, 2>(wa, pd, st, s, sh, tiles, seqP, seqC)
+                                   : team_propagator<KIND, 3>(wa, pd, st, s, sh, tiles, seqP, seqC);
+      if (lane == 0) sh->status = status;
+    } else {
+      if (pd.d == 2) team_helpers<KIND, 2>(wa, pd, st, s, sh, tiles, seqH, warp - 1);
+      else team_helpers<KIND, 3>(wa, pd, st, s, sh, tiles, seqH, warp - 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && sh->status == 0) {
+      const int S = (pd.n1 - 1 + 31) >> 5;
+      const unsigned long long ev = sh->evaluated;
+      if (ev) atomicAdd(KIND == K_DEC ? &st->cells_eval : &st->cells_vefd, ev);
+      __threadfence();
+      const int n = atomicAdd(&st->done_count, 1);
+      if (n == S - 1) {
+        __threadfence();
+        finalize<KIND>(st, pd, wa.active_pairs);
+        __threadfence();
+      }
+    }
+  }
+}
+
 // Per-pair constants and state.  One block per pair (grid-stride).
 __global__ void prep_kernel(const PairDesc* pairs, PairState* st, int npairs, int start_phase) {
   for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
@@ -244,6 +318,8 @@ struct rfd_context {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   int grid[3] = {0, 0, 0};
+  int team_grid[3] = {0, 0, 0};
+  int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
   void* dws = nullptr;
   size_t dws_size = 0;
   void* hws = nullptr;
@@ -519,14 +595,15 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     wave_kernel<K_DFD><<<ctx->grid[K_DFD], kBlock, 0, st>>>(wa);
     RFD_CUDA(cudaGetLastError());
     if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
-    wa.phase = PH_VEFD;
-    wa.ticket = counters + li++;
-    wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
-    RFD_CUDA(cudaGetLastError());
-    wa.phase = PH_VEFD_DENSE;
-    wa.ticket = counters + li++;
-    wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
-    RFD_CUDA(cudaGetLastError());
+    for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
+      wa.phase = ph;
+      wa.ticket = counters + li++;
+      if (ctx->solo)
+        wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
+      else
+        team_kernel<K_VEFD><<<ctx->team_grid[K_VEFD], kTeamThreads, team_smem_bytes<K_VEFD>(), st>>>(wa);
+      RFD_CUDA(cudaGetLastError());
+    }
     launches += 3;
   }
   if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
@@ -534,7 +611,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   for (int k = 0; k < nprobe; ++k) {
     wa.phase = PH_SEARCH;
     wa.ticket = counters + li++;
-    wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
+    if (ctx->solo)
+      wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
+    else
+      team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
     RFD_CUDA(cudaGetLastError());
     ++launches;
   }
@@ -651,6 +731,23 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], wave_kernel<K_VEFD>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], wave_kernel<K_DEC>, kBlock, 0);
   for (int k = 0; k < 3; ++k) c->grid[k] = std::max(1, occ[k]) * c->num_sms;
+  {
+    const size_t sm_ve = team_smem_bytes<K_VEFD>(), sm_dec = team_smem_bytes<K_DEC>();
+    if (cudaFuncSetAttribute(team_kernel<K_VEFD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm_ve) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_DEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm_dec) != cudaSuccess) {
+      delete c;
+      return fail(RFD_ERR_CUDA, "cudaFuncSetAttribute(team smem)");
+    }
+    int o1 = 0, o2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, team_kernel<K_VEFD>, kTeamThreads, sm_ve);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, team_kernel<K_DEC>, kTeamThreads, sm_dec);
+    c->team_grid[K_VEFD] = std::max(1, o1) * c->num_sms;
+    c->team_grid[K_DEC] = std::max(1, o2) * c->num_sms;
+    const char* e = getenv("RFD_SOLO");
+    c->solo = e && e[0] == '1';
+  }
   // wait budget: about 20 s at the maximum SM clock
   c->spin_cycles = (long long)prop.clockRate * 1000LL * 20LL;
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {

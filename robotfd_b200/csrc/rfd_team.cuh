@@ -1,0 +1,427 @@
+// "Team" strips: one CTA of 4 warps per 32-row strip for the VE-FD and decision DPs.
+//
+// The solo strip (rfd_device.cuh) computes each cell's geometry on the step-to-step
+// dependency chain, so a sparse band - a handful of live lanes per step - advances at the
+// latency of two FP64 quadratics per step.  Here the geometry leaves that chain:
+//   warps 1..3 (helpers)  compute a whole skewed 32x32 tile of step-chunk c - for the
+//                          decision the right and top free intervals of every cell, for
+//                          VE-FD the two vertex-edge weights - into shared memory;
+//   warp 0 (propagator)   runs the same skewed sweep, the same L2 strip handoff and the
+//                          same dead-region jumps as the solo strip, but a step is only a
+//                          shared-memory read, two shuffles and the min/max propagation.
+// Tile c+1 is requested speculatively while tile c is consumed (two slots, mbarrier
+// handshakes); a jump cancels the speculative tile.  The arithmetic of every cell is the
+// solo strip's (same functions), so results are bit-identical.
+#pragma once
+
+#include "rfd_device.cuh"
+
+namespace rfd {
+
+constexpr int kTeamThreads = 128;
+constexpr int kStop = -2;  // request word: strip finished
+
+struct TeamShared {
+  unsigned long long full[2];  // helpers -> propagator: tile ready (3 arrivals)
+  unsigned long long req[2];   // propagator -> helpers: chunk requested (1 arrival)
+  int req_chunk[2];
+  int cancel[2];
+  int item_pair, item_strip, go, quit;
+  unsigned long long evaluated;
+  int status;
+  int pad;
+};
+
+template <int KIND>
+struct TileT {
+  static constexpr int vals = KIND == K_DEC ? 2 : 1;  // double2 per cell
+  static constexpr size_t slot_bytes = (size_t)vals * 1024 * sizeof(double2);
+};
+
+template <int KIND>
+__host__ __device__ constexpr size_t team_smem_bytes() {
+  return 256 + 2 * TileT<KIND>::slot_bytes;
+}
+
+// ------------------------------------------------------------------ mbarrier helpers
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait (warp-uniform: every lane polls the same barrier phase).  false on timeout
+// or when the global error word is set.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, const WaveArgs& wa,
+                                          long long t0) {
+  for (int it = 0;; ++it) {
+    if (mbar_try_wait(b, parity)) return true;
+    if ((it & 63) == 63) {
+      int bad = 0;
+      if ((threadIdx.x & 31) == 0)
+        bad = ld_volatile(wa.error) || (clock64() - t0 > wa.spin_cycles);
+      if (__shfl_sync(kFull, bad, 0)) {
+        if ((threadIdx.x & 31) == 0) atomicExch(wa.error, 1);
+        return false;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ helpers (warps 1..3)
+
+template <int KIND, int D>
+__device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairState* st, int s,
+                             TeamShared* sh, double2* tiles, unsigned& seqH, int hw) {
+  const int lane = threadIdx.x & 31;
+  const int R = pd.n1 - 1, C = pd.n2 - 1;
+  const int i = (s << 5) + lane;
+  const bool rowv = i < R;
+  const double r2 = st->r2;
+  RowData<KIND, D> row;
+  if (rowv) row.load(pd, i);
+  const long long t0 = clock64();
+  unsigned long long count = 0;
+  for (;;) {
+    const int slot = seqH & 1;
+    if (!mbar_wait(&sh->req[slot], (seqH >> 1) & 1, wa, t0)) break;
+    const int c = *(volatile int*)&sh->req_chunk[slot];
+    if (c == kStop) {
+      // every request, the stop included, is answered with one completion, so the
+      // propagator's take count and the request count stay equal across strips
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh->full[slot]);
+      ++seqH;
+      break;
+    }
+    double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
+    double2* T1 = T0 + 1024;
+    for (int u = hw; u < 32; u += 3) {
+      if (__shfl_sync(kFull, *(volatile int*)&sh->cancel[slot], 0)) break;
+      const int j = (c << 5) + u - lane;
+      if (rowv && j >= 0 && j < C) {
+        ColRec<KIND, D> col;
+        load_col<KIND, D>(pd, j, col);
+        double qd[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) qd[k] = __dsub_rn(col.qb[k], col.qa[k]);
+        if (KIND == K_DEC) {
+          double rLB, rUB, tLB, tUB;
+          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
+          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+          T0[(u << 5) + lane] = make_double2(rLB, rUB);
+          T1[(u << 5) + lane] = make_double2(tLB, tUB);
+        } else {
+          const double wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
+          const double wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
+          T0[(u << 5) + lane] = make_double2(wt, wr);
+        }
+        ++count;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh->full[slot]);
+    ++seqH;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(kFull, count, o);
+  if (lane == 0 && count) atomicAdd(&sh->evaluated, count);
+}
+
+// ------------------------------------------------------------------ propagator (warp 0)
+
+template <int KIND, int D>
+__device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState* st, const int s,
+                               TeamShared* sh, const double2* tiles, unsigned& seqP,
+                               unsigned& seqC) {
+  const int lane = threadIdx.x & 31;
+  const int R = pd.n1 - 1;
+  const int C = pd.n2 - 1;
+  const int S = (R + 31) >> 5;
+  const unsigned E = st->epoch;
+  const double U = st->U;
+  const bool dense = st->dense != 0;
+  const bool has_prod = s > 0;
+  const bool has_cons = s + 1 < S;
+
+  Prog* in_prog = has_prod ? pd.prog + (s - 1) : nullptr;
+  Prog* out_prog = has_cons ? pd.prog + s : nullptr;
+  const double* in_bnd = has_prod ? pd.bnd + (size_t)(s - 1) * pd.cstride : nullptr;
+  double* out_bnd = has_cons ? pd.bnd + (size_t)s * pd.cstride : nullptr;
+  const unsigned* in_tags = has_prod ? pd.tags + (size_t)(s - 1) * pd.tstride : nullptr;
+  unsigned* out_tags = has_cons ? pd.tags + (size_t)s * pd.tstride : nullptr;
+
+  int status = 0;
+  Waiter wt;
+  wt.start(wa, st, s);
+  const long long t0 = clock64();
+
+  const int i = (s << 5) + lane;
+  const bool rowv = i < R;
+  const bool last_row = i == R - 1;
+  const int nout = (C + 31) >> 5;
+  const int nsteps = C + 31;
+  double res = KIND == K_DEC ? -2.0 : kFltMax;
+  bool dead_tail = !dense && bcast(lane == 0 ? ld_volatile(&st->dead_from) : 0) <= s;
+
+  if (has_cons && lane == 0) {
+    out_prog->first_live = kNone;
+    out_prog->last_live = 0;
+  }
+  double bot;
+  if (KIND == K_DEC) bot = i == 0 ? 0.0 : -1.0;
+  else bot = i == 0 ? st->seed : kFltMax;
+  double carry = dead_value<KIND>();
+  double ob0 = dead_value<KIND>(), ob1 = dead_value<KIND>();
+  unsigned first_live_out = kNone;
+  int next_flush = 0;
+  int pending = -1;  // chunk of the outstanding tile request (-1: none)
+
+  auto request = [&](int c) {
+    const int slot = seqP & 1;
+    if (lane == 0) {
+      *(volatile int*)&sh->req_chunk[slot] = c;
+      *(volatile int*)&sh->cancel[slot] = 0;
+      mbar_arrive(&sh->req[slot]);
+    }
+    __syncwarp();
+    ++seqP;
+  };
+  // Waits for the oldest outstanding tile; returns its slot or -1 on error.
+  auto take = [&]() -> int {
+    const int slot = seqC & 1;
+    if (!mbar_wait(&sh->full[slot], (seqC >> 1) & 1, wa, t0)) return -1;
+    ++seqC;
+    return slot;
+  };
+  auto drop_pending = [&]() -> bool {
+    if (pending < 0) return true;
+    if (lane == 0) *(volatile int*)&sh->cancel[seqC & 1] = 1;
+    __syncwarp();
+    pending = -1;
+    return take() >= 0;
+  };
+  auto flush = [&](int k) {
+    const int col = (k << 5) + lane;
+    double v = (k & 1) ? ob1 : ob0;
+    const bool valid = col < C;
+    if (valid) __stcg(out_bnd + col, v);
+    const unsigned live = __ballot_sync(kFull, valid && !is_dead<KIND>(v, U));
+    if (k & 1) ob1 = dead_value<KIND>();
+    else ob0 = dead_value<KIND>();
+    __syncwarp();
+    if (lane == 0) {
+      if (live) {
+        __stcg(out_tags + k, E);
+        if (first_live_out == kNone) {
+          first_live_out = (unsigned)k;
+          out_prog->first_live = (unsigned)k;
+        }
+        out_prog->last_live = (unsigned)k;
+      }
+      __threadfence();
+      st_release(&out_prog->word, ((unsigned long long)E << 32) | (unsigned)min((k + 1) << 5, C));
+    }
+  };
+  auto publish_cols = [&](int cols) {
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release(&out_prog->word, ((unsigned long long)E << 32) | (unsigned)cols);
+    }
+  };
+  auto wait_cols = [&](unsigned need, unsigned long long& w) -> int {
+    for (int it = 0;; ++it) {
+      w = bcast(lane == 0 ? ld_acquire(&in_prog->word) : 0ull);
+      if ((unsigned)(w >> 32) == E && (unsigned)(w & 0xffffffffu) >= need) return 0;
+      const int r = wt.check(it);
+      if (r) return r;
+    }
+  };
+
+  int c = 0;
+  while (!dead_tail && (c << 5) < nsteps) {
+    if (has_cons)
+      while (next_flush <= c - 2) flush(next_flush++);
+    double inreg = dead_value<KIND>();
+    bool in_live = false;
+    if ((c << 5) < C) {
+      if (has_prod) {
+        unsigned long long w;
+        const int r = wait_cols((unsigned)min((c + 1) << 5, C), w);
+        if (r == 2) { status = 1; break; }
+        if (r == 1) { dead_tail = true; break; }
+        const unsigned tg = bcast(lane == 0 ? __ldcg(in_tags + c) : 0u);
+        in_live = tg == E;
+        if (in_live) {
+          const int col = (c << 5) + lane;
+          if (col < C) inreg = __ldcg(in_bnd + col);
+        }
+      } else {
+        in_live = !is_dead<KIND>(inreg, U);
+      }
+    }
+    if (!dense && !in_live) {
+      const bool ldead = (!rowv || is_dead<KIND>(bot, U) || ((c << 5) - lane >= C)) &&
+                         is_dead<KIND>(carry, U);
+      if (__all_sync(kFull, ldead)) {
+        int nc = -1;
+        if (has_prod && (c << 5) < C) {
+          int pos = c + 1;
+          for (int it = 0;; ++it) {
+            unsigned long long w = 0ull;
+            unsigned fl = kNone, ll = 0u;
+            if (lane == 0) {
+              w = ld_acquire(&in_prog->word);
+              fl = __ldcg(&in_prog->first_live);
+              ll = __ldcg(&in_prog->last_live);
+            }
+            w = bcast(w);
+            fl = bcast(fl);
+            ll = bcast(ll);
+            const bool ours = (unsigned)(w >> 32) == E;
+            const unsigned cols = ours ? (unsigned)(w & 0xffffffffu) : 0u;
+            const bool done = ours && cols >= (unsigned)C;
+            if (!ours) fl = kNone;
+            const int avail = done ? nout : (int)(cols >> 5);
+            if (fl != kNone) {
+              pos = max(pos, (int)fl);
+              const int end = done ? min(nout, (int)ll + 1) : avail;
+              while (pos < end && nc < 0) {
+                const int k = pos + lane;
+                const bool hit = k < end && __ldcg(in_tags + k) == E;
+                const unsigned b = __ballot_sync(kFull, hit);
+                if (b) nc = pos + __ffs(b) - 1;
+                else pos = min(pos + 32, end);
+              }
+            } else {
+              pos = max(pos, avail);
+            }
+            if (nc >= 0 || done) break;
+            const int r = wt.check(it);
+            if (r == 2) { status = 1; break; }
+            if (r == 1) break;
+          }
+          if (status) break;
+        }
+        if (has_cons)
+          while (next_flush <= c - 1) flush(next_flush++);
+        if (!drop_pending()) { status = 1; break; }
+        if (nc < 0) {
+          dead_tail = true;
+          break;
+        }
+        if (has_cons) {
+          next_flush = nc - 1;
+          publish_cols(min((nc - 1) << 5, C));
+        }
+        carry = dead_value<KIND>();
+        ob0 = ob1 = dead_value<KIND>();
+        c = nc;
+        request(c);  // cold start of the live stretch
+        pending = c;
+        continue;
+      }
+    }
+    // ---- process step-chunk c from tile c
+    if (pending != c) {
+      if (!drop_pending()) { status = 1; break; }
+      request(c);
+      pending = c;
+    }
+    const int slot = take();
+    if (slot < 0) { status = 1; break; }
+    pending = -1;
+    if (((c + 1) << 5) < nsteps) {  // speculative: the next chunk is usually processed too
+      request(c + 1);
+      pending = c + 1;
+    }
+    const double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
+    const double2* T1 = T0 + 1024;
+#pragma unroll 4
+    for (int u = 0; u < 32; ++u) {
+      const int t = (c << 5) + u;
+      const double lin = __shfl_sync(kFull, inreg, u);
+      const double lup = __shfl_up_sync(kFull, carry, 1);
+      const double left = lane == 0 ? lin : lup;
+      const int j = t - lane;
+      const bool act = rowv && j >= 0 && j < C;
+      if (act) {
+        if (KIND == K_DEC) {
+          const double2 tr = T0[(u << 5) + lane], tt = T1[(u << 5) + lane];
+          double rLB = tr.x, rUB = tr.y, tLB = tt.x, tUB = tt.y;
+          const double leftLB = left, botLB = bot;
+          if (botLB < 0.0) {
+            const bool invalid = (leftLB > rUB) || (leftLB < 0.0);
+            const double m = fmax(rLB, leftLB);
+            rLB = invalid ? -1.0 : m;
+            rUB = invalid ? -2.0 : rUB;
+          }
+          if (leftLB < 0.0) {
+            const bool invalid = (botLB > tUB) || (botLB < 0.0);
+            const double m = fmax(tLB, botLB);
+            tLB = invalid ? -1.0 : m;
+            tUB = invalid ? -2.0 : tUB;
+          }
+          bot = tLB;
+          carry = rLB;
+          if (last_row && j == C - 1) res = rUB;
+        } else {
+          const double2 w = T0[(u << 5) + lane];
+          const double in = fmin(left, bot);
+          const double top = fmax(w.x, in);
+          const double right = fmax(w.y, in);
+          carry = right;
+          bot = top;
+          if (last_row && j == C - 1) res = fmin(top, right);
+        }
+      }
+      const double o = __shfl_sync(kFull, carry, 31);
+      const int jo = t - 31;
+      if (jo >= 0 && (jo & 31) == lane) {
+        if (jo & 32) ob1 = o;
+        else ob0 = o;
+      }
+    }
+    ++c;
+  }
+  if (status == 0 && !drop_pending()) status = 1;
+  // tell the helpers this strip is over (also after an error: they must not wait forever)
+  // and take their acknowledgement
+  if (lane == 0) {
+    const int slot = seqP & 1;
+    *(volatile int*)&sh->req_chunk[slot] = kStop;
+    mbar_arrive(&sh->req[slot]);
+  }
+  __syncwarp();
+  ++seqP;
+  if (take() < 0) status = 1;
+
+  if (status == 0 && has_cons) {
+    if (!dead_tail) {
+      while (next_flush < nout) flush(next_flush++);
+    } else {
+      publish_cols(C);
+    }
+    if (!dense && lane == 0 && first_live_out == kNone) atomicMin(&st->dead_from, s + 1);
+  }
+  if (s == S - 1 && last_row) st->result = res;
+  return status;
+}
+
+}  // namespace rfd

@@ -131,3 +131,47 @@ def test_sparse_equals_dense_large(ctx, built, style, d, n):
         assert sparse == dense, (e, sparse, dense)
     assert not ctx.decide(P, Q, fd * (1 - 1e-7))[0]
     assert ctx.decide(P, Q, fd * (1 + 1e-7))[0]
+
+
+@pytest.fixture(scope="module")
+def solo_ctx(built):
+    """A context whose VE-FD and decisions run on the one-warp strips (RFD_SOLO=1)."""
+    import os
+    old = os.environ.get("RFD_SOLO")
+    os.environ["RFD_SOLO"] = "1"
+    try:
+        c = built.Context(0)
+    finally:
+        if old is None:
+            del os.environ["RFD_SOLO"]
+        else:
+            os.environ["RFD_SOLO"] = old
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("style,d,n1,n2", [(0, 2, 700, 650), (1, 3, 3000, 2800), (0, 3, 97, 1300),
+                                           (1, 2, 1500, 40)])
+def test_team_equals_solo(ctx, solo_ctx, built, style, d, n1, n2):
+    """Helper-warp tiles (team strips) and on-chain geometry (solo strips) agree bit for bit."""
+    P, Q = built.gen_pair(style, d, n1, n2, 100.0 if style else 1.0, 0.1, 77, n1)
+    for dense in (False, True):
+        a = ctx.distance(P, Q, precise=True, dense=dense)
+        b = solo_ctx.distance(P, Q, precise=True, dense=dense)
+        for k in ("distance", "dfd", "vefd", "lb", "ub", "probes"):
+            assert a[k] == b[k], (k, dense, a[k], b[k])
+
+
+def test_reference_driver_golden(ctx, built):
+    """The CUDA path in the reference's configuration reproduces the reference's own search
+    driver (tests/golden/reference_host.json) bit for bit."""
+    import json
+    import os
+    from tests.golden.cases import build_input
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_host.json")) as f:
+        cases = json.load(f)["distance"]
+    for c in cases:
+        P, Q = build_input(c["input"])
+        r = ctx.distance(P, Q)
+        assert r["endpoint"] == c["endpoint"], c["name"]
+        assert r["distance"] == c["distance"], c["name"]
