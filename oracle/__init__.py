@@ -4,8 +4,9 @@ Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench
 may import this package, as the checker or the timed CPU baseline; the product
 (``robotfd_b200``) never calls it.  The C source ``rfd_oracle.c`` restates the
 reference's DFD, VE-FD and fused-decision cells and its epsilon search (file:line
-citations in its header).  Parity is pinned by mathematical known-answer tests and by
-outputs of the reference's own GPU code run on the same inputs (``tests/golden``).
+citations in its header).  Its search driver, endpoint bound and the loaders are pinned by
+the reference's own host code run on the same inputs (``tests/golden``); its cells by
+mathematical known-answer tests and brute-force definitions (``tests/test_oracle.py``).
 """
 import ctypes
 import os

@@ -24,9 +24,12 @@
  * bound and the bisection midpoint are host arithmetic in the reference (g++, no FMA) and
  * are restated without fusion.
  *
- * Parity pin: the reference has no tests or golden data; the oracle is pinned by
- * mathematical known-answer tests and by outputs of the reference's own GPU code run on
- * the same inputs (tests/golden/, made by oracle/refharness/).
+ * Parity pin: the reference has no tests or golden data.  The search driver, stop rule,
+ * endpoint bound and loaders are pinned by the reference's own host code run on the same
+ * inputs (tests/golden/reference_host.json, made through oracle/refharness/); the DFD,
+ * VE-FD and decision cells by mathematical known-answer tests and independent
+ * brute-force definitions (tests/test_oracle.py).  They are not pinned to outputs of the
+ * reference's GPU kernels, which are not run here.
  */
 #include <float.h>
 #include <math.h>

@@ -86,6 +86,7 @@ struct WaveArgs {
   int* error;
   int* active_pairs;
   long long spin_cycles;
+  unsigned long long* prof;  // RFD_PROF=1: cycle counters (see rfd_team.cuh), else null
 };
 
 // ------------------------------------------------------------------ memory helpers

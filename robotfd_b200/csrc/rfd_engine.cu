@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int k = 0; k < 2; ++k) {
-      mbar_init(&sh->full[k], 3);
+      mbar_init(&sh->full[k], kHelpers);
       mbar_init(&sh->req[k], 1);
     }
   }
@@ -320,6 +320,7 @@ struct rfd_context {
   int grid[3] = {0, 0, 0};
   int team_grid[3] = {0, 0, 0};
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
+  int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
   size_t dws_size = 0;
   void* hws = nullptr;
@@ -438,6 +439,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0);
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * L.nlaunch);
+  const size_t prof_off = take(sizeof(unsigned long long) * 16);
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
@@ -587,6 +589,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   wa.error = (int*)(dbase + L.error);
   wa.active_pairs = (int*)(dbase + L.active);
   wa.spin_cycles = ctx->spin_cycles;
+  wa.prof = ctx->prof ? (unsigned long long*)(dbase + prof_off) : nullptr;
   unsigned* counters = (unsigned*)(dbase + L.counters);
   int li = 0;
   if (mode != MODE_DECIDE) {
@@ -625,6 +628,15 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   RFD_CUDA(cudaMemcpyAsync(hmisc + 1, wa.error, sizeof(int), cudaMemcpyDeviceToHost, st));
   RFD_CUDA(cudaStreamSynchronize(st));
   if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
+  if (ctx->prof) {
+    unsigned long long pc[16];
+    RFD_CUDA(cudaMemcpy(pc, dbase + prof_off, sizeof(pc), cudaMemcpyDeviceToHost));
+    fprintf(stderr,
+            "rfd prof (Mcycles): in_wait %.1f jump %.1f tile_wait %.1f steps %.1f strip_total %.1f |"
+            " chunks %llu jumps %llu strips %llu | helpers: tile %.1f req_wait %.1f tiles %llu\n",
+            pc[0] / 1e6, pc[1] / 1e6, pc[2] / 1e6, pc[3] / 1e6, pc[4] / 1e6, pc[5], pc[6], pc[7],
+            pc[8] / 1e6, pc[9] / 1e6, pc[10]);
+  }
   if (ctx->timing) {
     float a = 0.f, b = 0.f, c = 0.f;
     if (mode != MODE_DECIDE) {
@@ -747,6 +759,8 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     c->team_grid[K_DEC] = std::max(1, o2) * c->num_sms;
     const char* e = getenv("RFD_SOLO");
     c->solo = e && e[0] == '1';
+    const char* pe = getenv("RFD_PROF");
+    c->prof = pe && pe[0] == '1';
   }
   // wait budget: about 20 s at the maximum SM clock
   c->spin_cycles = (long long)prop.clockRate * 1000LL * 20LL;

@@ -18,11 +18,12 @@
 
 namespace rfd {
 
-constexpr int kTeamThreads = 128;
+constexpr int kTeamThreads = 256;
+constexpr int kHelpers = kTeamThreads / 32 - 1;  // helper warps per team
 constexpr int kStop = -2;  // request word: strip finished
 
 struct TeamShared {
-  unsigned long long full[2];  // helpers -> propagator: tile ready (3 arrivals)
+  unsigned long long full[2];  // helpers -> propagator: tile ready (kHelpers arrivals)
   unsigned long long req[2];   // propagator -> helpers: chunk requested (1 arrival)
   int req_chunk[2];
   int cancel[2];
@@ -99,7 +100,9 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
   unsigned long long count = 0;
   for (;;) {
     const int slot = seqH & 1;
+    const long long tw0 = wa.prof ? clock64() : 0;
     if (!mbar_wait(&sh->req[slot], (seqH >> 1) & 1, wa, t0)) break;
+    if (wa.prof && lane == 0) atomicAdd(&wa.prof[9], (unsigned long long)(clock64() - tw0));
     const int c = *(volatile int*)&sh->req_chunk[slot];
     if (c == kStop) {
       // every request, the stop included, is answered with one completion, so the
@@ -111,28 +114,43 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     }
     double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
     double2* T1 = T0 + 1024;
-    for (int u = hw; u < 32; u += 3) {
-      if (__shfl_sync(kFull, *(volatile int*)&sh->cancel[slot], 0)) break;
+    const long long tc0 = wa.prof ? clock64() : 0;
+    // Two independent cells (u, u + kHelpers) per iteration, their records loaded with
+    // clamped indices so no load waits on a branch; results are stored only for cells
+    // inside the grid.
+    auto one = [&](int u, const ColRec<KIND, D>& col) {
       const int j = (c << 5) + u - lane;
-      if (rowv && j >= 0 && j < C) {
-        ColRec<KIND, D> col;
-        load_col<KIND, D>(pd, j, col);
-        double qd[D];
+      double qd[D];
 #pragma unroll
-        for (int k = 0; k < D; ++k) qd[k] = __dsub_rn(col.qb[k], col.qa[k]);
-        if (KIND == K_DEC) {
-          double rLB, rUB, tLB, tUB;
-          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
-          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+      for (int k = 0; k < D; ++k) qd[k] = __dsub_rn(col.qb[k], col.qa[k]);
+      const bool ok = rowv && j >= 0 && j < C;
+      if (KIND == K_DEC) {
+        double rLB, rUB, tLB, tUB;
+        free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
+        free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+        if (ok) {
           T0[(u << 5) + lane] = make_double2(rLB, rUB);
           T1[(u << 5) + lane] = make_double2(tLB, tUB);
-        } else {
-          const double wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
-          const double wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
-          T0[(u << 5) + lane] = make_double2(wt, wr);
         }
-        ++count;
+      } else {
+        const double wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
+        const double wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
+        if (ok) T0[(u << 5) + lane] = make_double2(wt, wr);
       }
+      count += ok ? 1 : 0;
+    };
+    for (int u0 = hw; u0 < 32; u0 += 2 * kHelpers) {
+      if (__shfl_sync(kFull, *(volatile int*)&sh->cancel[slot], 0)) break;
+      const int u1 = u0 + kHelpers;
+      ColRec<KIND, D> c0, c1;
+      load_col<KIND, D>(pd, min(max((c << 5) + u0 - lane, 0), C - 1), c0);
+      load_col<KIND, D>(pd, min(max((c << 5) + min(u1, 31) - lane, 0), C - 1), c1);
+      one(u0, c0);
+      if (u1 < 32) one(u1, c1);
+    }
+    if (wa.prof && lane == 0) {
+      atomicAdd(&wa.prof[8], (unsigned long long)(clock64() - tc0));
+      atomicAdd(&wa.prof[10], 1ull);
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&sh->full[slot]);
@@ -170,6 +188,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   Waiter wt;
   wt.start(wa, st, s);
   const long long t0 = clock64();
+  if (wa.prof && lane == 0) atomicAdd(&wa.prof[7], 1ull);
 
   const int i = (s << 5) + lane;
   const bool rowv = i < R;
@@ -205,7 +224,9 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // Waits for the oldest outstanding tile; returns its slot or -1 on error.
   auto take = [&]() -> int {
     const int slot = seqC & 1;
+    const long long tw0 = wa.prof ? clock64() : 0;
     if (!mbar_wait(&sh->full[slot], (seqC >> 1) & 1, wa, t0)) return -1;
+    if (wa.prof && lane == 0) atomicAdd(&wa.prof[2], (unsigned long long)(clock64() - tw0));
     ++seqC;
     return slot;
   };
@@ -246,9 +267,13 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
   };
   auto wait_cols = [&](unsigned need, unsigned long long& w) -> int {
+    const long long tw0 = wa.prof ? clock64() : 0;
     for (int it = 0;; ++it) {
       w = bcast(lane == 0 ? ld_acquire(&in_prog->word) : 0ull);
-      if ((unsigned)(w >> 32) == E && (unsigned)(w & 0xffffffffu) >= need) return 0;
+      if ((unsigned)(w >> 32) == E && (unsigned)(w & 0xffffffffu) >= need) {
+        if (wa.prof && lane == 0) atomicAdd(&wa.prof[0], (unsigned long long)(clock64() - tw0));
+        return 0;
+      }
       const int r = wt.check(it);
       if (r) return r;
     }
@@ -283,6 +308,9 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         int nc = -1;
         if (has_prod && (c << 5) < C) {
           int pos = c + 1;
+          const long long tj0 = wa.prof ? clock64() : 0;
+          // the speculative tile in flight (chunk c) is not needed: the warp skips c
+          if (!drop_pending()) { status = 1; break; }
           for (int it = 0;; ++it) {
             unsigned long long w = 0ull;
             unsigned fl = kNone, ll = 0u;
@@ -309,6 +337,13 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
                 if (b) nc = pos + __ffs(b) - 1;
                 else pos = min(pos + 32, end);
               }
+              // The producer's first live chunk at or after pos is where this strip will
+              // most likely resume: start its tile now so it is ready at the jump.
+              if (nc < 0 && pos < nout && pending != pos) {
+                if (!drop_pending()) { status = 1; break; }
+                request(pos);
+                pending = pos;
+              }
             } else {
               pos = max(pos, avail);
             }
@@ -318,10 +353,19 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
             if (r == 1) break;
           }
           if (status) break;
+          if (wa.prof && lane == 0) {
+            atomicAdd(&wa.prof[1], (unsigned long long)(clock64() - tj0));
+            atomicAdd(&wa.prof[6], 1ull);
+          }
         }
         if (has_cons)
           while (next_flush <= c - 1) flush(next_flush++);
-        if (!drop_pending()) { status = 1; break; }
+        if (nc >= 0 && pending == nc) {
+          // the speculative cold-start tile is the one we need: keep it
+        } else if (!drop_pending()) {
+          status = 1;
+          break;
+        }
         if (nc < 0) {
           dead_tail = true;
           break;
@@ -333,8 +377,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         carry = dead_value<KIND>();
         ob0 = ob1 = dead_value<KIND>();
         c = nc;
-        request(c);  // cold start of the live stretch
-        pending = c;
+        if (pending != c) {
+          request(c);  // cold start of the live stretch
+          pending = c;
+        }
         continue;
       }
     }
@@ -353,50 +399,49 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
     const double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
     const double2* T1 = T0 + 1024;
-#pragma unroll 4
+    const long long ts0 = wa.prof ? clock64() : 0;
+#pragma unroll
     for (int u = 0; u < 32; ++u) {
-      const int t = (c << 5) + u;
+      // tile reads and the input broadcast do not depend on the previous step
+      const double2 ta = T0[(u << 5) + lane];
+      const double2 tb = KIND == K_DEC ? T1[(u << 5) + lane] : ta;
       const double lin = __shfl_sync(kFull, inreg, u);
       const double lup = __shfl_up_sync(kFull, carry, 1);
       const double left = lane == 0 ? lin : lup;
-      const int j = t - lane;
+      const int j = (c << 5) + u - lane;
       const bool act = rowv && j >= 0 && j < C;
-      if (act) {
-        if (KIND == K_DEC) {
-          const double2 tr = T0[(u << 5) + lane], tt = T1[(u << 5) + lane];
-          double rLB = tr.x, rUB = tr.y, tLB = tt.x, tUB = tt.y;
-          const double leftLB = left, botLB = bot;
-          if (botLB < 0.0) {
-            const bool invalid = (leftLB > rUB) || (leftLB < 0.0);
-            const double m = fmax(rLB, leftLB);
-            rLB = invalid ? -1.0 : m;
-            rUB = invalid ? -2.0 : rUB;
-          }
-          if (leftLB < 0.0) {
-            const bool invalid = (botLB > tUB) || (botLB < 0.0);
-            const double m = fmax(tLB, botLB);
-            tLB = invalid ? -1.0 : m;
-            tUB = invalid ? -2.0 : tUB;
-          }
-          bot = tLB;
-          carry = rLB;
-          if (last_row && j == C - 1) res = rUB;
-        } else {
-          const double2 w = T0[(u << 5) + lane];
-          const double in = fmin(left, bot);
-          const double top = fmax(w.x, in);
-          const double right = fmax(w.y, in);
-          carry = right;
-          bot = top;
-          if (last_row && j == C - 1) res = fmin(top, right);
-        }
+      double ncarry, nbot, nres;
+      if (KIND == K_DEC) {
+        // same propagation as the solo cell, written with selects (no divergence)
+        const double rLB = ta.x, rUB = ta.y, tLB = tb.x, tUB = tb.y;
+        const bool bdead = bot < 0.0, ldead = left < 0.0;
+        const bool rinv = (left > rUB) || ldead;
+        const bool tinv = (bot > tUB) || bdead;
+        const double rm = fmax(rLB, left);
+        const double tm = fmax(tLB, bot);
+        ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
+        nres = bdead ? (rinv ? -2.0 : rUB) : rUB;
+        nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
+      } else {
+        const double in = fmin(left, bot);
+        const double top = fmax(ta.x, in);
+        const double right = fmax(ta.y, in);
+        ncarry = right;
+        nbot = top;
+        nres = fmin(top, right);
       }
+      carry = act ? ncarry : carry;
+      bot = act ? nbot : bot;
+      if (act && last_row && j == C - 1) res = nres;
       const double o = __shfl_sync(kFull, carry, 31);
-      const int jo = t - 31;
-      if (jo >= 0 && (jo & 31) == lane) {
-        if (jo & 32) ob1 = o;
+      if (lane == ((u + 1) & 31)) {  // lane 31 produced column (c << 5) + u - 31
+        if (((((c << 5) + u - 31) >> 5) & 1) != 0) ob1 = o;
         else ob0 = o;
       }
+    }
+    if (wa.prof && lane == 0) {
+      atomicAdd(&wa.prof[3], (unsigned long long)(clock64() - ts0));
+      atomicAdd(&wa.prof[5], 1ull);
     }
     ++c;
   }
@@ -421,6 +466,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     if (!dense && lane == 0 && first_live_out == kNone) atomicMin(&st->dead_from, s + 1);
   }
   if (s == S - 1 && last_row) st->result = res;
+  if (wa.prof && lane == 0) atomicAdd(&wa.prof[4], (unsigned long long)(clock64() - t0));
   return status;
 }
 
