@@ -145,6 +145,22 @@ int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double*
 int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
                    int32_t dims, double radius, int32_t dense, int32_t* reachable, double* right_ub);
 
+/* One reachability decision that allocates nothing (no counterpart in the reference).
+   For callers that cannot allocate device memory once they run: a robot's control loop
+   where an allocation could stall for an unbounded time or fail when the GPU is full, or
+   a process sharing the GPU under a memory budget fixed at start-up.  The curves (c1, c2)
+   and the output (right_ub, one double) are the caller's device memory; all other working
+   memory is one file-scope device array of 64 MiB that every GPU loading librfd.so holds
+   until exit (pairs needing more return RFD_ERR_LIMIT before anything runs).  The work is
+   enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the call returns
+   without waiting: *right_ub receives the propagated right UB of the last cell (reachable
+   iff it equals 1.0), or NaN if an inter-warp wait timed out.  The first call on a device
+   looks up the array's address and sets kernel attributes there, so make that first call
+   before any stream capture.  All calls share the array and each clears what must start
+   at zero; calls whose work overlaps on the GPU race and must not be issued. */
+int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double* c2, int64_t n2,
+                           int32_t dims, double radius, void* stream, double* right_ub);
+
 /* ---- loader ----
    Text curve loader: one point per line, comma separated, consecutive duplicates dropped.
    Replaces txtLoader2 / txtLoader3 (include/txtReader.hpp:6, :48).  On success *out is a

@@ -51,7 +51,7 @@ EXPORTS = (
     "rfd_context_create", "rfd_context_destroy", "rfd_context_set_stream",
     "rfd_context_phase_times", "rfd_fp64_peak", "rfd_distance",
     "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_load_txt", "rfd_free",
-    "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step",
+    "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
 )
 
 
@@ -151,6 +151,8 @@ def lib():
     L.rfd_gen_batch_spec.restype = i32
     L.rfd_search_step.argtypes = [_dp, _i32p, i32, i32, dbl, i32, _dp]
     L.rfd_search_step.restype = i32
+    L.rfd_decide_noalloc.argtypes = [vp, i64, vp, i64, i32, dbl, vp, vp]
+    L.rfd_decide_noalloc.restype = i32
     _LIB = L
     return L
 
@@ -383,3 +385,11 @@ def search_step(state, istate, stop_mode, have_outcome, eps, reachable):
     more = lib().rfd_search_step(st, ist, stop_mode, int(bool(have_outcome)), float(eps),
                                  int(bool(reachable)), ctypes.byref(nxt))
     return bool(more), nxt.value, list(st), list(ist)
+
+
+def decide_noalloc(p_dev, n1, q_dev, n2, dims, radius, stream, out_dev):
+    """rfd_decide_noalloc on device pointers: enqueues one decision on `stream` and writes
+    the propagated right UB of the last cell to out_dev (one double, device memory)."""
+    _check(lib().rfd_decide_noalloc(ctypes.c_void_p(p_dev), int(n1), ctypes.c_void_p(q_dev),
+                                    int(n2), int(dims), float(radius), ctypes.c_void_p(stream),
+                                    ctypes.c_void_p(out_dev)))

@@ -11,6 +11,7 @@
 //           pair's probe applies the outcome and proposes the next radius on the device
 //           (reference host loop src/frechet.cpp:36-63)
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include <algorithm>
 #include <cfloat>
@@ -18,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -914,3 +916,152 @@ int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32
 }
 
 }  // extern "C"
+
+// ============================================================================ no-allocation decision
+//
+// rfd_decide_noalloc: one reachability decision for callers that cannot allocate device
+// memory at call time - a robot's control loop that must not allocate once it runs (an
+// allocation can stall for an unbounded time or fail when the GPU is full), or a process
+// that shares the GPU under a fixed memory budget reserved at start-up.  Everything the
+// decision needs beyond the caller's inputs and output lives in one file-scope device
+// array of kNoAllocBytes, which every GPU that loads this library holds until the process
+// exits.  Calls share that array: a call clears what must start at zero, and two calls
+// whose work overlaps on the GPU (different streams, or different host threads) race on it.
+
+namespace {
+
+constexpr size_t kNoAllocBytes = (size_t)64 << 20;  // 64 MiB
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocDevice {
+  int ready;
+  unsigned char* scratch;  // device address of g_noalloc_scratch on this device
+  int team_grid;
+  long long spin_cycles;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc[64];
+
+__global__ void noalloc_setup_kernel(PairDesc* desc, PairState* st, int2* items, int nitems,
+                                     int* active, PairDesc d, double radius, double r2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    *desc = d;
+    PairState s;
+    memset(&s, 0, sizeof(s));
+    s.srch.tol = 0.0;
+    s.srch.stop_mode = RFD_STOP_ABS;
+    s.decide_only = 1;
+    s.split = radius;
+    s.r2 = r2;
+    s.blo = s.bhi = CUDART_NAN;
+    *st = s;
+    *active = 1;
+  }
+  for (int k = t; k < nitems; k += gridDim.x * blockDim.x) items[k] = make_int2(0, k);
+}
+
+__global__ void noalloc_emit_kernel(const PairState* st, const int* error, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = *error ? CUDART_NAN : st->result;
+}
+
+}  // namespace
+
+extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double* c2, int64_t n2,
+                                      int32_t dims, double radius, void* stream,
+                                      double* right_ub) {
+  if (!c1 || !c2 || !right_ub) return fail(RFD_ERR_ARG, "null pointer");
+  if (dims != 2 && dims != 3) return fail(RFD_ERR_ARG, "dims must be 2 or 3");
+  if (n1 < 2 || n2 < 2) return fail(RFD_ERR_ARG, "decisions need curves of at least two points");
+  if (!(radius >= 0.0)) return fail(RFD_ERR_ARG, "radius");
+  int dev = 0;
+  RFD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(RFD_ERR_ARG, "device index above 63");
+  {
+    // once per device, with that device current: the array's device address and the
+    // launch attributes of the decision kernel
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice& nd = g_noalloc[dev];
+    if (!nd.ready) {
+      void* p = nullptr;
+      RFD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      const size_t sm_dec = team_smem_bytes<K_DEC>();
+      RFD_CUDA(cudaFuncSetAttribute(team_kernel<K_DEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sm_dec));
+      int occ = 0, nsm = 0, clk = 0;
+      RFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, team_kernel<K_DEC>, kTeamThreads,
+                                                             sm_dec));
+      RFD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      RFD_CUDA(cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, dev));
+      nd.scratch = (unsigned char*)p;
+      nd.team_grid = std::max(1, occ) * nsm;
+      nd.spin_cycles = (long long)clk * 1000LL * 20LL;
+      nd.ready = 1;
+    }
+  }
+  const NoAllocDevice nd = g_noalloc[dev];
+  // layout inside the array (same records as the allocating path)
+  const int64_t S = (n1 + 31) / 32;
+  const int64_t cstride = (int64_t)align_up((size_t)n2, 32);
+  const int64_t tstride = (int64_t)align_up((size_t)((n2 + 31) / 32), 32);
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t r = off; off = align_up(off + bytes, 256); return r; };
+  const size_t o_desc = take(sizeof(PairDesc));
+  const size_t o_state = take(sizeof(PairState));
+  const size_t o_items = take(sizeof(int2) * S);
+  const size_t o_zero = off;
+  const size_t o_ticket = take(sizeof(unsigned));
+  const size_t o_error = take(sizeof(int));
+  const size_t o_tags = take(sizeof(unsigned) * (size_t)(S - 1) * tstride);
+  const size_t o_prog = take(sizeof(Prog) * S);
+  const size_t zero_end = off;
+  const size_t o_active = take(sizeof(int));
+  const size_t o_rowc = take(sizeof(double2) * (size_t)(n1 - 1));
+  const size_t o_colrec = take(sizeof(double2) * (dims == 2 ? 3 : 4) * (size_t)(n2 - 1));
+  const size_t o_bnd = take(sizeof(double) * (size_t)(S - 1) * cstride);
+  if (off > kNoAllocBytes)
+    return fail(RFD_ERR_LIMIT, "rfd_decide_noalloc: the pair needs " + std::to_string(off) +
+                                   " bytes of scratch, the fixed array holds " +
+                                   std::to_string(kNoAllocBytes));
+  unsigned char* base = nd.scratch;
+  PairDesc d;
+  memset(&d, 0, sizeof(d));
+  d.P = c1;
+  d.Q = c2;
+  d.rowc = (const double2*)(base + o_rowc);
+  d.colrec = (const double2*)(base + o_colrec);
+  d.bnd = (double*)(base + o_bnd);
+  d.tags = (unsigned*)(base + o_tags);
+  d.prog = (Prog*)(base + o_prog);
+  d.n1 = (int)n1;
+  d.n2 = (int)n2;
+  d.d = dims;
+  d.cstride = cstride;
+  d.tstride = tstride;
+  cudaStream_t st = (cudaStream_t)stream;
+  PairDesc* ddesc = (PairDesc*)(base + o_desc);
+  PairState* dstate = (PairState*)(base + o_state);
+  RFD_CUDA(cudaMemsetAsync(base + o_zero, 0, zero_end - o_zero, st));
+  noalloc_setup_kernel<<<(int)std::min<int64_t>((S + 255) / 256, 64) + 1, 256, 0, st>>>(
+      ddesc, dstate, (int2*)(base + o_items), (int)S, (int*)(base + o_active), d, radius,
+      radius * radius);
+  RFD_CUDA(cudaGetLastError());
+  prep_kernel<<<1, 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH);
+  RFD_CUDA(cudaGetLastError());
+  WaveArgs wa;
+  wa.pairs = ddesc;
+  wa.st = dstate;
+  wa.items = (const int2*)(base + o_items);
+  wa.nitems = (int)S;
+  wa.phase = PH_SEARCH;
+  wa.ticket = (unsigned*)(base + o_ticket);
+  wa.error = (int*)(base + o_error);
+  wa.active_pairs = (int*)(base + o_active);
+  wa.spin_cycles = nd.spin_cycles;
+  wa.prof = nullptr;
+  team_kernel<K_DEC><<<nd.team_grid, kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+  RFD_CUDA(cudaGetLastError());
+  noalloc_emit_kernel<<<1, 32, 0, st>>>(dstate, wa.error, right_ub);
+  RFD_CUDA(cudaGetLastError());
+  return RFD_OK;
+}
