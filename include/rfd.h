@@ -59,6 +59,8 @@ enum rfd_flag {
   RFD_FLAG_DEGENERATE = 128    /* a curve of one point: closed form used */
 };
 
+typedef struct rfd_model rfd_model;
+
 typedef struct rfd_options {
   int32_t stop_mode;        /* enum rfd_stop */
   int32_t reference_quirks; /* 1: reproduce the reference's VE-FD launch rule
@@ -70,6 +72,8 @@ typedef struct rfd_options {
   int32_t memory;           /* where curve pointers live: enum rfd_memory */
   const double* bracket;    /* optional, 2 doubles per pair: proposed [lo, hi] containing the
                                distance; verified by two decisions, widened on failure */
+  const rfd_model* model;   /* optional learned bracket: proposes [lo, hi] per pair from the
+                               curves and the VE-FD bound (ignored when bracket is set) */
 } rfd_options;
 
 typedef struct rfd_result {
@@ -160,6 +164,36 @@ int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double*
    at zero; calls whose work overlaps on the GPU race and must not be issued. */
 int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double* c2, int64_t n2,
                            int32_t dims, double radius, void* stream, double* right_ub);
+
+/* ---- learned bracket (no reference counterpart) ----
+   A BF16 MLP (400 -> 256 -> 256 -> 256 -> 2, GELU, FP32 accumulation) on the tensor cores,
+   predicting the 5% and 95% quantiles of log10(FD / VEFD - 1 + 1e-13) from bracket
+   features.  Parameters are one flat FP32 array of rfd_model_num_params() values (layer
+   by layer: W[out][in] row-major then b[out]).  x/t/y pointers are device memory. */
+int64_t rfd_model_num_params(void);
+int32_t rfd_model_create(int32_t device, uint64_t seed, rfd_model** out);
+int32_t rfd_model_destroy(rfd_model* model);
+int32_t rfd_model_set_params(rfd_model* model, const float* params, int64_t n);
+int32_t rfd_model_get_params(rfd_model* model, float* params, int64_t n);
+/* y[B][2] = model(x[B][400]) */
+int32_t rfd_model_forward(rfd_model* model, const float* x, int64_t B, float* y);
+/* pinball loss of x[B][400] against targets t[B]; grads (host, num_params floats) may be NULL */
+int32_t rfd_model_gradients(rfd_model* model, const float* x, const float* t, int64_t B,
+                            float* grads, float* loss);
+/* one Adam step (beta 0.9 / 0.999) on the pinball loss of a minibatch */
+int32_t rfd_model_train_step(rfd_model* model, const float* x, const float* t, int64_t B,
+                             float lr, float* loss);
+/* The network's GEMM kernel on its own (test entry): C[M][N] = A[M][K] B[K][N] with
+   A(m,k) = A[m*a_sr + k*a_sc], B(k,n) = B[k*b_sr + n*b_sc], operands rounded to BF16,
+   FP32 accumulation; all pointers device memory. */
+int32_t rfd_gemm_bf16(int32_t M, int32_t N, int32_t K, const float* A, int64_t a_sr, int64_t a_sc,
+                      const float* B, int64_t b_sr, int64_t b_sc, float* C);
+/* Bracket features of npairs pairs (host curves, endpoint and VE-FD bounds) into
+   out[npairs][400] (host): both curves resampled to 64 points uniform in arc length,
+   centred and scaled, then log(endpoint / scale) and log(VEFD / scale), zero padded. */
+int32_t rfd_features(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
+                     const double* const* c2s, const int64_t* n2s, const int32_t* dims,
+                     const double* endpoint, const double* vefd, float* out);
 
 /* ---- loader ----
    Text curve loader: one point per line, comma separated, consecutive duplicates dropped.

@@ -52,6 +52,9 @@ EXPORTS = (
     "rfd_context_phase_times", "rfd_fp64_peak", "rfd_distance",
     "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_load_txt", "rfd_free",
     "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
+    "rfd_model_num_params", "rfd_model_create", "rfd_model_destroy", "rfd_model_set_params",
+    "rfd_model_get_params", "rfd_model_forward", "rfd_model_gradients", "rfd_model_train_step",
+    "rfd_features", "rfd_gemm_bf16",
 )
 
 
@@ -71,6 +74,7 @@ class Options(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("memory", ctypes.c_int32),
         ("bracket", ctypes.POINTER(ctypes.c_double)),
+        ("model", ctypes.c_void_p),
     ]
 
 
@@ -153,6 +157,27 @@ def lib():
     L.rfd_search_step.restype = i32
     L.rfd_decide_noalloc.argtypes = [vp, i64, vp, i64, i32, dbl, vp, vp]
     L.rfd_decide_noalloc.restype = i32
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.rfd_model_num_params.restype = i64
+    L.rfd_model_create.argtypes = [i32, ctypes.c_uint64, ctypes.POINTER(vp)]
+    L.rfd_model_create.restype = i32
+    L.rfd_model_destroy.argtypes = [vp]
+    L.rfd_model_destroy.restype = i32
+    L.rfd_model_set_params.argtypes = [vp, fp, i64]
+    L.rfd_model_set_params.restype = i32
+    L.rfd_model_get_params.argtypes = [vp, fp, i64]
+    L.rfd_model_get_params.restype = i32
+    L.rfd_model_forward.argtypes = [vp, vp, i64, vp]
+    L.rfd_model_forward.restype = i32
+    L.rfd_model_gradients.argtypes = [vp, vp, vp, i64, fp, fp]
+    L.rfd_model_gradients.restype = i32
+    L.rfd_model_train_step.argtypes = [vp, vp, vp, i64, ctypes.c_float, fp]
+    L.rfd_model_train_step.restype = i32
+    L.rfd_features.argtypes = [vp, i64, ctypes.POINTER(vp), _i64p, ctypes.POINTER(vp), _i64p, _i32p,
+                               _dp, _dp, fp]
+    L.rfd_features.restype = i32
+    L.rfd_gemm_bf16.argtypes = [i32, i32, i32, vp, i64, i64, vp, i64, i64, vp]
+    L.rfd_gemm_bf16.restype = i32
     _LIB = L
     return L
 
@@ -177,7 +202,7 @@ def _curve(c):
 
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
-            precision=RFD_PREC_FP64):
+            precision=RFD_PREC_FP64, model=None):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -188,6 +213,8 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
         o.tol = float(tol)
     if quirks is not None:
         o.reference_quirks = int(bool(quirks))
+    if model is not None:
+        o.model = model._h.value
     return o
 
 
@@ -219,6 +246,24 @@ class Context:
         _check(lib().rfd_context_phase_times(self._h, int(enable), out))
         return dict(zip(("dfd_ms", "vefd_ms", "search_ms", "calls", "launches", "h2d_bytes",
                          "d2h_bytes"), list(out)))
+
+    def features(self, Ps, Qs, endpoint, vefd):
+        """Bracket features [npairs][400] (float32) of host curves (rfd_features)."""
+        n = len(Ps)
+        keep = [_curve(x) for x in Ps] + [_curve(x) for x in Qs]
+        A, B = keep[:n], keep[n:]
+        p1 = (ctypes.c_void_p * n)(*[a.ctypes.data for a in A])
+        p2 = (ctypes.c_void_p * n)(*[b.ctypes.data for b in B])
+        n1 = (ctypes.c_int64 * n)(*[len(a) for a in A])
+        n2 = (ctypes.c_int64 * n)(*[len(b) for b in B])
+        dm = (ctypes.c_int32 * n)(*[a.shape[1] for a in A])
+        ep = np.ascontiguousarray(endpoint, dtype=np.float64)
+        ve = np.ascontiguousarray(vefd, dtype=np.float64)
+        out = np.zeros((n, FEATURE_WIDTH), dtype=np.float32)
+        _check(lib().rfd_features(self._h, n, p1, n1, p2, n2, dm, ep.ctypes.data_as(_dp),
+                                  ve.ctypes.data_as(_dp),
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
 
     def fp64_peak(self):
         """Measured FP64 FMA throughput in TFLOP/s."""
@@ -393,3 +438,73 @@ def decide_noalloc(p_dev, n1, q_dev, n2, dims, radius, stream, out_dev):
     _check(lib().rfd_decide_noalloc(ctypes.c_void_p(p_dev), int(n1), ctypes.c_void_p(q_dev),
                                     int(n2), int(dims), float(radius), ctypes.c_void_p(stream),
                                     ctypes.c_void_p(out_dev)))
+
+
+FEATURE_WIDTH = 400
+N_FEATURES = 386
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+class Model:
+    """The learned-bracket network (rfd_model): BF16 MLP 400-256-256-256-2 on one GPU."""
+
+    def __init__(self, device=0, seed=0, params=None):
+        h = ctypes.c_void_p()
+        _check(lib().rfd_model_create(int(device), ctypes.c_uint64(seed), ctypes.byref(h)))
+        self._h = h
+        self.device = device
+        if params is not None:
+            self.set_params(params)
+
+    @staticmethod
+    def num_params():
+        return int(lib().rfd_model_num_params())
+
+    def close(self):
+        if self._h:
+            lib().rfd_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        _check(lib().rfd_model_set_params(self._h, p.ctypes.data_as(_fp), p.size))
+
+    def get_params(self):
+        p = np.empty(self.num_params(), dtype=np.float32)
+        _check(lib().rfd_model_get_params(self._h, p.ctypes.data_as(_fp), p.size))
+        return p
+
+    def forward(self, x_dev, B, y_dev):
+        _check(lib().rfd_model_forward(self._h, ctypes.c_void_p(x_dev), int(B), ctypes.c_void_p(y_dev)))
+
+    def gradients(self, x_dev, t_dev, B):
+        g = np.empty(self.num_params(), dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().rfd_model_gradients(self._h, ctypes.c_void_p(x_dev), ctypes.c_void_p(t_dev),
+                                         int(B), g.ctypes.data_as(_fp), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, x_dev, t_dev, B, lr):
+        loss = ctypes.c_float()
+        _check(lib().rfd_model_train_step(self._h, ctypes.c_void_p(x_dev), ctypes.c_void_p(t_dev),
+                                          int(B), ctypes.c_float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def save(self, path):
+        np.save(path, self.get_params())
+
+    @classmethod
+    def load(cls, path, device=0):
+        return cls(device=device, params=np.load(path))
+
+
+def gemm_bf16(M, N, K, a_ptr, a_sr, a_sc, b_ptr, b_sr, b_sc, c_ptr):
+    """The network's GEMM kernel alone (device pointers, FP32 operands rounded to BF16)."""
+    _check(lib().rfd_gemm_bf16(M, N, K, ctypes.c_void_p(a_ptr), a_sr, a_sc, ctypes.c_void_p(b_ptr),
+                               b_sr, b_sc, ctypes.c_void_p(c_ptr)))

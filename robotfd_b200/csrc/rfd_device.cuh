@@ -35,7 +35,14 @@ constexpr unsigned kNone = 0xffffffffu;
 constexpr unsigned kFull = 0xffffffffu;
 
 enum Kind : int { K_DFD = 0, K_VEFD = 1, K_DEC = 2 };
-enum Phase : int { PH_DFD = 0, PH_VEFD = 1, PH_VEFD_DENSE = 2, PH_SEARCH = 3, PH_DONE = 4 };
+enum Phase : int {
+  PH_DFD = 0,
+  PH_VEFD = 1,
+  PH_VEFD_DENSE = 2,
+  PH_SEARCH = 3,
+  PH_DONE = 4,
+  PH_BRACKET = 5  // waiting for the learned bracket
+};
 
 // Progress record of a strip's output boundary.
 struct Prog {
@@ -68,7 +75,8 @@ struct PairState {
   unsigned int epoch;
   int phase, active, quirks, dense, decide_only, flags;
   int dead_from, done_count;
-  int pad[3];
+  int use_model;
+  int pad[2];
 };
 
 template <int D>

@@ -26,6 +26,8 @@
 #include "rfd.h"
 #include "rfd_device.cuh"
 #include "rfd_team.cuh"
+#include "rfd_features.cuh"
+#include "rfd_mlp.h"
 
 using namespace rfd;
 
@@ -38,6 +40,14 @@ int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+}  // namespace
+
+int rfd_mlp::set_error(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
+namespace {
 
 #define RFD_CUDA(call)                                                                    \
   do {                                                                                    \
@@ -90,7 +100,8 @@ __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
       if (st->quirks && prod <= 10000) {
         st->vefd = st->endpoint;
         st->flags |= RFD_FLAG_VEFD_SKIPPED;
-        begin_search(st, active_pairs);
+        if (st->use_model) st->phase = PH_BRACKET;
+        else begin_search(st, active_pairs);
       } else {
         st->phase = PH_VEFD;
         // VE-FD <= CFD <= DFD; the margin absorbs rounding when they coincide.
@@ -104,7 +115,8 @@ __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
       st->flags |= RFD_FLAG_VEFD_DENSE;
     } else {
       st->vefd = __dsqrt_rn(r);  // reference .cu:427
-      begin_search(st, active_pairs);
+      if (st->use_model) st->phase = PH_BRACKET;
+      else begin_search(st, active_pairs);
     }
   } else {
     st->cells_nominal += (unsigned long long)(pd.n1 - 1) * (unsigned long long)(pd.n2 - 1);
@@ -232,6 +244,52 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
         __threadfence();
       }
     }
+  }
+}
+
+// Learned bracket, step 1: features of every pair waiting in PH_BRACKET (one CTA each).
+__global__ void __launch_bounds__(kFeatThreads) bracket_features_kernel(const PairDesc* pairs,
+                                                                       const PairState* st,
+                                                                       int npairs, float* feat) {
+  __shared__ FeatScratch sh;
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    float* out = feat + (size_t)p * rfd_mlp::kInputWidth;
+    if (st[p].phase != PH_BRACKET) {
+      for (int f = threadIdx.x; f < rfd_mlp::kInputWidth; f += blockDim.x) out[f] = 0.f;
+      continue;
+    }
+    const PairDesc pd = pairs[p];
+    pair_features(pd.P, pd.n1, pd.Q, pd.n2, pd.d, st[p].endpoint, st[p].vefd, sh, out);
+  }
+}
+
+// Learned bracket, step 2: q = model quantiles of log10(FD/VEFD - 1 + 1e-13); bracket
+// [VEFD (1 + 10^q05), VEFD (1 + 10^q95)], then the verified search starts.
+__global__ void bracket_apply_kernel(PairState* st, int npairs, const float* y, int* active_pairs) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+    PairState* s = st + p;
+    if (s->phase != PH_BRACKET) continue;
+    double qlo = fmin(1.0, fmax(-13.0, (double)y[2 * p]));
+    double qhi = fmin(1.0, fmax(-13.0, (double)y[2 * p + 1]));
+    if (qhi < qlo) {
+      const double tq = qlo;
+      qlo = qhi;
+      qhi = tq;
+    }
+    s->blo = s->vefd * (1.0 + exp10(qlo));
+    s->bhi = s->vefd * (1.0 + exp10(qhi));
+    begin_search(s, active_pairs);
+  }
+}
+
+__global__ void __launch_bounds__(kFeatThreads) features_kernel(const PairDesc* pairs, int npairs,
+                                                               const double* endpoint,
+                                                               const double* vefd, float* feat) {
+  __shared__ FeatScratch sh;
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const PairDesc pd = pairs[p];
+    pair_features(pd.P, pd.n1, pd.Q, pd.n2, pd.d, endpoint[p], vefd[p], sh,
+                  feat + (size_t)p * rfd_mlp::kInputWidth);
   }
 }
 
@@ -453,6 +511,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   }
   L.zero_end = off;
   L.active = take(sizeof(int));
+  const bool use_model = mode == MODE_DISTANCE && o.model && !o.bracket;
+  const size_t feat_off = use_model ? take(sizeof(float) * rfd_mlp::kInputWidth * npairs) : 0;
+  const size_t y_off = use_model ? take(sizeof(float) * rfd_mlp::kOutputs * npairs) : 0;
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
     const int d = dims[p];
@@ -527,6 +588,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     s.srch.max_probes = max_probes;
     s.quirks = o.reference_quirks;
     s.dense = o.dense;
+    s.use_model = use_model ? 1 : 0;
     s.blo = s.bhi = NAN;
     if (o.bracket && mode == MODE_DISTANCE) {
       s.blo = o.bracket[2 * p];
@@ -610,6 +672,22 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       RFD_CUDA(cudaGetLastError());
     }
     launches += 3;
+    if (use_model) {
+      rfd_model* md = const_cast<rfd_model*>(o.model);
+      if (rfd_mlp::model_device(md) != ctx->device)
+        return fail(RFD_ERR_ARG, "the model lives on another device");
+      float* feat = (float*)(dbase + feat_off);
+      float* yout = (float*)(dbase + y_off);
+      bracket_features_kernel<<<(int)std::min<int64_t>(npairs, 16 * ctx->num_sms), kFeatThreads, 0,
+                                st>>>(dd, ds, (int)npairs, feat);
+      RFD_CUDA(cudaGetLastError());
+      int rc2 = rfd_mlp::infer(md, feat, (int)npairs, yout, st);
+      if (rc2) return rc2;
+      bracket_apply_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
+          ds, (int)npairs, yout, wa.active_pairs);
+      RFD_CUDA(cudaGetLastError());
+      launches += 2 + 4;
+    }
   }
   if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
   const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
@@ -884,6 +962,62 @@ int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double*
   if (rc) return rc;
   *reachable = r.distance == 1.0;
   if (right_ub) *right_ub = r.distance;
+  return RFD_OK;
+}
+
+int32_t rfd_features(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
+                     const double* const* c2s, const int64_t* n2s, const int32_t* dims,
+                     const double* endpoint, const double* vefd, float* out) {
+  if (!ctx || npairs < 0 || !c1s || !n1s || !c2s || !n2s || !dims || !endpoint || !vefd || !out)
+    return fail(RFD_ERR_ARG, "null argument");
+  if (npairs == 0) return RFD_OK;
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  size_t bytes = 0;
+  std::vector<size_t> o1(npairs), o2(npairs);
+  for (int64_t p = 0; p < npairs; ++p) {
+    int rc = check_pair(c1s[p], n1s[p], c2s[p], n2s[p], dims[p]);
+    if (rc) return rc;
+    if (n1s[p] < 2 || n2s[p] < 2) return fail(RFD_ERR_ARG, "features need curves of two points");
+    o1[p] = bytes;
+    bytes = align_up(bytes + sizeof(double) * n1s[p] * dims[p], 256);
+    o2[p] = bytes;
+    bytes = align_up(bytes + sizeof(double) * n2s[p] * dims[p], 256);
+  }
+  const size_t o_desc = bytes;
+  bytes = align_up(bytes + sizeof(PairDesc) * npairs, 256);
+  const size_t o_ep = bytes;
+  bytes = align_up(bytes + sizeof(double) * npairs, 256);
+  const size_t o_ve = bytes;
+  bytes = align_up(bytes + sizeof(double) * npairs, 256);
+  const size_t o_feat = bytes;
+  bytes = align_up(bytes + sizeof(float) * rfd_mlp::kInputWidth * npairs, 256);
+  int rc = ensure_device(ctx, bytes);
+  if (rc) return rc;
+  char* base = (char*)ctx->dws;
+  std::vector<PairDesc> hd(npairs);
+  cudaStream_t st = ctx->stream;
+  for (int64_t p = 0; p < npairs; ++p) {
+    memset(&hd[p], 0, sizeof(PairDesc));
+    hd[p].P = (const double*)(base + o1[p]);
+    hd[p].Q = (const double*)(base + o2[p]);
+    hd[p].n1 = (int)n1s[p];
+    hd[p].n2 = (int)n2s[p];
+    hd[p].d = dims[p];
+    RFD_CUDA(cudaMemcpyAsync(base + o1[p], c1s[p], sizeof(double) * n1s[p] * dims[p],
+                             cudaMemcpyHostToDevice, st));
+    RFD_CUDA(cudaMemcpyAsync(base + o2[p], c2s[p], sizeof(double) * n2s[p] * dims[p],
+                             cudaMemcpyHostToDevice, st));
+  }
+  RFD_CUDA(cudaMemcpyAsync(base + o_desc, hd.data(), sizeof(PairDesc) * npairs, cudaMemcpyHostToDevice, st));
+  RFD_CUDA(cudaMemcpyAsync(base + o_ep, endpoint, sizeof(double) * npairs, cudaMemcpyHostToDevice, st));
+  RFD_CUDA(cudaMemcpyAsync(base + o_ve, vefd, sizeof(double) * npairs, cudaMemcpyHostToDevice, st));
+  features_kernel<<<(int)std::min<int64_t>(npairs, 16 * ctx->num_sms), kFeatThreads, 0, st>>>(
+      (const PairDesc*)(base + o_desc), (int)npairs, (const double*)(base + o_ep),
+      (const double*)(base + o_ve), (float*)(base + o_feat));
+  RFD_CUDA(cudaGetLastError());
+  RFD_CUDA(cudaMemcpyAsync(out, base + o_feat, sizeof(float) * rfd_mlp::kInputWidth * npairs,
+                           cudaMemcpyDeviceToHost, st));
+  RFD_CUDA(cudaStreamSynchronize(st));
   return RFD_OK;
 }
 
