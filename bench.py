@@ -35,6 +35,9 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
             "20-knot time warp, noise 0.1, seed 1); FD to 2^-33 relative")
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
+DEC_DRAM_BYTES_20K = 2.408192e6
+KERNEL_OF_PHASE = {"dfd": "wave_kernel<K_DFD>", "vefd": "team_kernel<K_VEFD>",
+                   "search": "team_kernel<K_DEC>"}
 FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3, "vefd": lambda d: 24 * d + 2,
                   "search": lambda d: 12 * d + 22}
 
@@ -45,8 +48,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=12000,
+    ap.add_argument("--cpu-sample", type=int, default=60000,
                     help="points per curve of the CPU-baseline sample")
+    ap.add_argument("--points", type=int, default=200000,
+                    help="points per curve of the long pair (smaller values: profiling cases)")
     return ap.parse_args()
 
 
@@ -111,9 +116,12 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload():
+def workload(points=200000):
+    """The long pair; other sizes keep its generator (waypoints = points / 100, seed 1)."""
     import robotfd_b200 as rfd
-    return rfd.gen_config(1)[0]
+    if points == 200000:
+        return rfd.gen_config(1)[0]
+    return rfd.gen_pair(1, 3, points, points, 100.0, 0.1, 1, 0)
 
 
 def cpu_sample(P, Q, m, probes):
@@ -148,7 +156,7 @@ def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    P, Q = workload()
+    P, Q = workload(args.points)
     probes = 37  # decisions of this workload's solve at 2^-33 (identical decisions as the GPU)
     vals = []
     for k in range(args.warmup + args.steps):
@@ -184,7 +192,7 @@ def main():
     ctx = rfd.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    P, Q = workload()
+    P, Q = workload(args.points)
     n1, n2, d = len(P), len(Q), P.shape[1]
     dP = torch.from_numpy(P).cuda()
     dQ = torch.from_numpy(Q).cuda()
@@ -255,10 +263,12 @@ def main():
     flops = cells[dom] * FLOPS_PER_CELL[dom](d)
     achieved = flops / (ph_ms[dom] * 1e-3) / 1e12
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get(dom)
+    if dom == "search":
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum of one decision launch on the
+        # 20,000-point case (cold cache: every touched point record and boundary word once);
+        # the touched data grows with the points, not the cells, so it scales by n1 + n2
+        traffic = DEC_DRAM_BYTES_20K * (n1 + n2) / 40000
+    sm_mhz = clk.get("sm_mhz") or 1965.0
 
     line = {
         "metric": METRIC,
@@ -273,7 +283,8 @@ def main():
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n1": n1, "n2": n2, "dims": d,
+        "config": {"workload": WORKLOAD if args.points == 200000 else
+                   f"long-pair generator at {args.points} points per curve", "n1": n1, "n2": n2, "dims": d,
                    "stop": "ub-lb <= 2^-33 ub", "parallelism": f"replicas x{world}",
                    "l2": "flushed before every step (256 MiB write outside the timed events)"},
         "fd": res["distance"],
@@ -287,11 +298,20 @@ def main():
                                "vefd_nominal": (n1 - 1) * (n2 - 1) / (ph_ms["vefd"] * 1e-3),
                                "vefd_evaluated": res["cells_vefd"] / (ph_ms["vefd"] * 1e-3)},
         "phase_ms": ph_ms,
-        "roofline": {"bound": "fp64", "kernel": f"wave_kernel<{dom}>", "achieved": achieved,
+        "roofline": {"bound": "fp64", "kernel": KERNEL_OF_PHASE[dom], "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic,
                      "peak_source": "measured FP64 FMA throughput (rfd_fp64_peak), this GPU",
-                     "flops_per_cell": FLOPS_PER_CELL[dom](d), "cells": cells[dom]},
+                     "flops_per_cell": FLOPS_PER_CELL[dom](d), "cells": cells[dom],
+                     "traffic_note": "bytes per launch, ncu cold-cache capture at 20k points "
+                                     "scaled by points"},
+        # the decision is bound by its dependency chain, not by flops or bytes: the wavefront
+        # has n1 + n2 anti-diagonals, so this is the latency each one adds to a probe
+        "critical_path": {
+            "antidiagonals": n1 + n2,
+            "ms_per_probe": ph_ms["search"] / max(res["probes"], 1),
+            "cycles_per_antidiagonal": ph_ms["search"] / max(res["probes"], 1) * 1e-3
+                                       * sm_mhz * 1e6 / (n1 + n2)},
         "e2e": {"value": e2e_value, "unit": "solves/s",
                 "h2d_bytes_per_step": ephase["h2d_bytes"] / max(ephase["calls"], 1),
                 "d2h_bytes_per_step": ephase["d2h_bytes"] / max(ephase["calls"], 1)},

@@ -169,7 +169,9 @@ int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double* c2, int64
    A BF16 MLP (400 -> 256 -> 256 -> 256 -> 2, GELU, FP32 accumulation) on the tensor cores,
    predicting the 5% and 95% quantiles of log10(FD / VEFD - 1 + 1e-13) from bracket
    features.  Parameters are one flat FP32 array of rfd_model_num_params() values (layer
-   by layer: W[out][in] row-major then b[out]).  x/t/y pointers are device memory. */
+   by layer: W[out][in] row-major then b[out]).  x/t/y pointers are device memory.  The
+   model works on its own stream: x and t must be complete on the device when a call is
+   made (synchronise the producing stream first); each call returns after its work ends. */
 int64_t rfd_model_num_params(void);
 int32_t rfd_model_create(int32_t device, uint64_t seed, rfd_model** out);
 int32_t rfd_model_destroy(rfd_model* model);

@@ -1,0 +1,211 @@
+"""Training and evaluation of the learned bracket network.
+
+Pairs come from the uneven-batch generator (lognormal lengths, median 2,000 points, sigma 1,
+clipped to [100, 50,000]; 2D/3D and walk/spline shapes 50/50).  Each pair is labelled by the
+plain method on the GPU (endpoint bound, DFD, VE-FD, bisection to 2^-33), its bracket
+features come from rfd_features (the same device code the solver uses), and the target is
+y = log10(FD / VEFD - 1 + 1e-13).  The network is trained on the GPU by its own forward and
+backward kernels (rfd_model_train_step: pinball loss of the 5% / 95% quantiles, Adam).
+
+Training runs on standardised inputs and targets; afterwards both affine maps are folded into
+the first and last layers, so the saved parameters take the solver's raw features.
+
+    python -m robotfd_b200.train_bracket [--pairs 200000] [--seed 3] [--eval-pairs 4096]
+        [--eval-seed 4] [--epochs 40] [--out robotfd_b200/bracket_model.npy]
+
+prints one JSON object: training set, loss curve, and the held-out evaluation (probes with
+and without the network, verification failures, solves/s, largest deviation from plain).
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+if __package__ in (None, ""):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import robotfd_b200 as rfd  # noqa: E402
+
+CONFIG = 3          # uneven-batch generator (training and held-out pairs differ by seed)
+CHUNK = 4096        # pairs per labelling call
+TOL = 2.0 ** -33    # precise stop rule: ub - lb <= 2^-33 ub
+DEFAULT_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bracket_model.npy")
+
+
+def target(res):
+    """y = log10(FD/VEFD - 1 + 1e-13); NaN where VE-FD is missing (degenerate pairs)."""
+    fd, ve = res["distance"], res["vefd"]
+    if not (ve > 0 and fd == fd) or res["flags"] & rfd.FLAG_DEGENERATE:
+        return np.nan
+    return float(np.log10(max(fd / ve - 1.0, 0.0) + 1e-13))
+
+
+def pairs_of(npairs, seed, start, stop):
+    dims, n1, n2, styles, scales, noises = rfd.gen_batch_spec(CONFIG, npairs, seed)
+    return [rfd.gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]), float(scales[k]),
+                         float(noises[k]), seed, k) for k in range(start, stop)]
+
+
+def label(ctx, npairs, seed, log=None):
+    """Features [npairs][400] (float32), targets [npairs] and the plain results' probes."""
+    X = np.zeros((npairs, rfd.FEATURE_WIDTH), np.float32)
+    y = np.full(npairs, np.nan)
+    probes = np.zeros(npairs, np.int32)
+    t0 = time.perf_counter()
+    for s in range(0, npairs, CHUNK):
+        e = min(npairs, s + CHUNK)
+        pairs = pairs_of(npairs, seed, s, e)
+        Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+        res = ctx.distance_batch(Ps, Qs, precise=True)
+        ep = np.array([r["endpoint"] for r in res])
+        ve = np.array([r["vefd"] for r in res])
+        ok = ve > 0
+        if ok.any():
+            idx = np.nonzero(ok)[0]
+            X[s + idx] = ctx.features([Ps[i] for i in idx], [Qs[i] for i in idx], ep[idx], ve[idx])
+        y[s:e] = [target(r) for r in res]
+        probes[s:e] = [r["probes"] for r in res]
+        if log:
+            log(f"labelled {e}/{npairs} pairs, {time.perf_counter() - t0:.1f} s")
+    return X, y, probes
+
+
+def fold(params, mu, sd, ymu, ysd):
+    """Folds x -> (x - mu) / sd into layer 1 and y -> y * ysd + ymu into layer 4."""
+    p = params.astype(np.float64).copy()
+    n_in, h = rfd.FEATURE_WIDTH, 256
+    W1 = p[: h * n_in].reshape(h, n_in)
+    b1 = p[h * n_in: h * n_in + h]
+    b1 -= W1 @ (mu / sd)
+    W1 /= sd[None, :]
+    o4 = len(p) - (2 * h + 2)
+    W4 = p[o4: o4 + 2 * h].reshape(2, h)
+    b4 = p[o4 + 2 * h:]
+    W4 *= ysd
+    b4[:] = b4 * ysd + ymu
+    return p.astype(np.float32)
+
+
+def train(X, y, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
+    """Trains a fresh network on (X, y); returns it with the normalisations folded in."""
+    import torch
+    ok = np.isfinite(y)
+    X, y = X[ok], y[ok]
+    mu = X.mean(0).astype(np.float64)
+    sd = X.std(0).astype(np.float64)
+    sd[sd < 1e-6] = 1.0
+    mu[sd == 1.0] = 0.0
+    ymu, ysd = float(np.median(y)), float(max(y.std(), 1e-3))
+    Xn = ((X - mu) / sd).astype(np.float32)
+    yn = ((y - ymu) / ysd).astype(np.float32)
+    dX = torch.from_numpy(Xn).to(f"cuda:{device}")
+    dy = torch.from_numpy(yn).to(f"cuda:{device}")
+    model = rfd.Model(device, seed=seed)
+    gen = torch.Generator(device=f"cuda:{device}").manual_seed(seed)
+    n = len(y)
+    steps_per_epoch = max(1, n // batch)
+    total = epochs * steps_per_epoch
+    losses, step = [], 0
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=gen, device=dX.device)
+        acc = 0.0
+        for k in range(steps_per_epoch):
+            idx = perm[k * batch:(k + 1) * batch]
+            xb, yb = dX[idx].contiguous(), dy[idx].contiguous()
+            # the network runs on its own stream: the gathers must be complete first
+            torch.cuda.current_stream().synchronize()
+            cur = lr * 0.5 * (1 + np.cos(np.pi * step / total)) + 1e-5
+            acc += model.train_step(xb.data_ptr(), yb.data_ptr(), len(idx), cur)
+            step += 1
+        losses.append(acc / steps_per_epoch * ysd)
+        if log:
+            log(f"epoch {ep + 1}/{epochs}: pinball loss {losses[-1]:.4f}")
+    model.set_params(fold(model.get_params(), mu, sd, ymu, ysd))
+    return model, losses
+
+
+def evaluate(ctx, model, npairs, seed, log=None):
+    """Held-out pairs solved with and without the network."""
+    stats = {"pairs": npairs, "plain_probes": 0, "learned_probes": 0, "plain_s": 0.0,
+             "learned_s": 0.0, "widened": 0, "one_probe": 0, "max_rel_dev": 0.0,
+             "max_rel_gap": 0.0}
+    for s in range(0, npairs, CHUNK):
+        e = min(npairs, s + CHUNK)
+        pairs = pairs_of(npairs, seed, s, e)
+        Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+        ctx.distance_batch(Ps[:8], Qs[:8], precise=True)  # workspace sized, kernels loaded
+        t0 = time.perf_counter()
+        plain = ctx.distance_batch(Ps, Qs, precise=True)
+        t1 = time.perf_counter()
+        got = ctx.distance_batch(Ps, Qs, precise=True, model=model)
+        t2 = time.perf_counter()
+        stats["plain_s"] += t1 - t0
+        stats["learned_s"] += t2 - t1
+        for a, b in zip(plain, got):
+            stats["plain_probes"] += a["probes"]
+            stats["learned_probes"] += b["probes"]
+            stats["widened"] += bool(b["flags"] & rfd.FLAG_BRACKET_WIDENED)
+            stats["one_probe"] += b["probes"] <= 1
+            if a["distance"] > 0:
+                stats["max_rel_dev"] = max(stats["max_rel_dev"],
+                                           abs(a["distance"] - b["distance"]) / a["distance"])
+                stats["max_rel_gap"] = max(stats["max_rel_gap"], (b["ub"] - b["lb"]) / b["ub"])
+        if log:
+            log(f"evaluated {e}/{npairs} pairs")
+    n = npairs
+    return {
+        "pairs": n,
+        "mean_probes_plain": stats["plain_probes"] / n,
+        "mean_probes_learned": stats["learned_probes"] / n,
+        "probes_saved_fraction": 1 - stats["learned_probes"] / max(stats["plain_probes"], 1),
+        "bracket_verification_failure_rate": stats["widened"] / n,
+        "one_probe_fraction": stats["one_probe"] / n,
+        "solves_per_s_plain": n / stats["plain_s"],
+        "solves_per_s_learned": n / stats["learned_s"],
+        "max_rel_deviation_from_plain": stats["max_rel_dev"],
+        "max_rel_final_gap": stats["max_rel_gap"],
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=200000)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--eval-pairs", type=int, default=4096)
+    ap.add_argument("--eval-seed", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    args = ap.parse_args(argv)
+
+    def log(m):
+        print(m, file=sys.stderr, flush=True)
+
+    ctx = rfd.Context(args.device)
+    t0 = time.perf_counter()
+    X, y, probes = label(ctx, args.pairs, args.seed, log)
+    t_label = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    model, losses = train(X, y, args.epochs, lr=args.lr, device=args.device, log=log)
+    t_train = time.perf_counter() - t0
+    model.save(args.out)
+    fin = y[np.isfinite(y)]
+    out = {
+        "train": {"pairs": args.pairs, "seed": args.seed, "usable": int(fin.size),
+                  "label_s": t_label, "train_s": t_train, "epochs": args.epochs,
+                  "mean_plain_probes": float(probes.mean()),
+                  "y_quantiles": {q: float(np.quantile(fin, q)) for q in (0.05, 0.5, 0.95, 0.99)},
+                  "loss_first": losses[0], "loss_last": losses[-1]},
+        "eval": evaluate(ctx, model, args.eval_pairs, args.eval_seed, log),
+        "out": os.path.relpath(args.out),
+    }
+    print(json.dumps(out), flush=True)
+    model.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
