@@ -214,8 +214,10 @@ int32_t rfd_gen_batch_spec(int32_t config, int64_t npairs, uint64_t seed, int32_
 
 /* ---- search state machine (host-callable copy of the device logic, for tests) ----
    Applies one decision outcome to a bracket search and proposes the next probe.
-   state[0..5] = {lb, ub, lo, hi, tol, unused}, istate[0..3] = {mode, probes, max_probes, flags},
-   stop_mode as in rfd_options.  Returns 1 and *next_eps when another probe is due. */
+   state[0..5] = {lb, ub, lo, hi, tol, t}, istate[0..3] = {mode, probes, max_probes, flags},
+   stop_mode as in rfd_options.  Returns 1 and *next_eps when another probe is due.  The first
+   call (probes 0, no outcome) starts the search as the device does: a finite bracket lo < hi
+   enables its checks, and t receives the stop threshold above lb, probed first when lo < t. */
 int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32_t have_outcome,
                         double eps, int32_t reachable, double* next_eps);
 

@@ -503,6 +503,13 @@ class Model:
     def load(cls, path, device=0):
         return cls(device=device, params=np.load(path))
 
+    @classmethod
+    def pretrained(cls, device=0):
+        """The network shipped with the package (robotfd_b200/bracket_model.npy), trained by
+        robotfd_b200/train_bracket.py on uneven-batch pairs labelled by the plain method."""
+        return cls.load(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                     "bracket_model.npy"), device)
+
 
 def gemm_bf16(M, N, K, a_ptr, a_sr, a_sc, b_ptr, b_sr, b_sc, c_ptr):
     """The network's GEMM kernel alone (device pointers, FP32 operands rounded to BF16)."""

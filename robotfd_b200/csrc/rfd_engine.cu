@@ -57,7 +57,8 @@ namespace {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                    \
   } while (0)
 
-__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs);
+__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs,
+                                             bool threshold_first);
 __device__ __forceinline__ void next_probe(PairState* st, int* active_pairs);
 
 __device__ __forceinline__ void finish_pair(PairState* st, int* active_pairs) {
@@ -78,9 +79,13 @@ __device__ __forceinline__ void next_probe(PairState* st, int* active_pairs) {
   }
 }
 
-__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs) {
+// threshold_first: the bracket comes from the learned network, which is trained on the
+// pairs whose distance lies above the stop threshold over VE-FD (the others end at the
+// threshold probe, which the search therefore always tries first).
+__device__ __forceinline__ void begin_search(PairState* st, int* active_pairs,
+                                             bool threshold_first) {
   if (st->vefd > st->dfd) st->flags |= RFD_FLAG_LB_GT_UB;
-  search_begin(st->srch, st->vefd, st->dfd, st->blo, st->bhi);
+  search_begin(st->srch, st->vefd, st->dfd, st->blo, st->bhi, threshold_first);
   next_probe(st, active_pairs);
 }
 
@@ -101,7 +106,7 @@ __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
         st->vefd = st->endpoint;
         st->flags |= RFD_FLAG_VEFD_SKIPPED;
         if (st->use_model) st->phase = PH_BRACKET;
-        else begin_search(st, active_pairs);
+        else begin_search(st, active_pairs, false);
       } else {
         st->phase = PH_VEFD;
         // VE-FD <= CFD <= DFD; the margin absorbs rounding when they coincide.
@@ -116,7 +121,7 @@ __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
     } else {
       st->vefd = __dsqrt_rn(r);  // reference .cu:427
       if (st->use_model) st->phase = PH_BRACKET;
-      else begin_search(st, active_pairs);
+      else begin_search(st, active_pairs, false);
     }
   } else {
     st->cells_nominal += (unsigned long long)(pd.n1 - 1) * (unsigned long long)(pd.n2 - 1);
@@ -278,7 +283,7 @@ __global__ void bracket_apply_kernel(PairState* st, int npairs, const float* y, 
     }
     s->blo = s->vefd * (1.0 + exp10(qlo));
     s->bhi = s->vefd * (1.0 + exp10(qhi));
-    begin_search(s, active_pairs);
+    begin_search(s, active_pairs, true);
   }
 }
 
@@ -1034,7 +1039,10 @@ int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32
   s.probes = istate[1];
   s.max_probes = istate[2];
   s.flags = istate[3];
+  s.t = state[5];
   s.stop_mode = stop_mode;
+  // the first call starts the search as the device does (bracket checks, threshold probe)
+  if (!have_outcome && s.probes == 0) search_begin(s, s.lb, s.ub, s.lo, s.hi);
   if (have_outcome) search_update(s, eps, reachable != 0);
   double e = 0.0;
   const int more = search_next(s, &e) ? 1 : 0;
@@ -1042,6 +1050,7 @@ int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32
   state[1] = s.ub;
   state[2] = s.lo;
   state[3] = s.hi;
+  state[5] = s.t;
   istate[0] = s.mode;
   istate[1] = s.probes;
   istate[3] = s.flags;

@@ -7,11 +7,19 @@ features come from rfd_features (the same device code the solver uses), and the 
 y = log10(FD / VEFD - 1 + 1e-13).  The network is trained on the GPU by its own forward and
 backward kernels (rfd_model_train_step: pinball loss of the 5% / 95% quantiles, Adam).
 
+VE-FD is a lower bound that equals FD within the 2^-33 stop tolerance for most pairs (97% of
+this generator's), and the search always tries the threshold probe VE-FD (1 + 0.999 2^-33)
+first when it has the network's bracket: those pairs end in one probe whatever the network
+says.  The network's bracket is used only after that probe fails, so it is trained on the
+pairs above the threshold (their y is also the only part of the label the plain method's
+stop rule resolves: below it, y is the search's stopping noise).
+
 Training runs on standardised inputs and targets; afterwards both affine maps are folded into
 the first and last layers, so the saved parameters take the solver's raw features.
 
     python -m robotfd_b200.train_bracket [--pairs 200000] [--seed 3] [--eval-pairs 4096]
-        [--eval-seed 4] [--epochs 40] [--out robotfd_b200/bracket_model.npy]
+        [--eval-seed 4] [--epochs 150] [--out robotfd_b200/bracket_model.npy]
+    python -m robotfd_b200.train_bracket --eval-only robotfd_b200/bracket_model.npy
 
 prints one JSON object: training set, loss curve, and the held-out evaluation (probes with
 and without the network, verification failures, solves/s, largest deviation from plain).
@@ -31,6 +39,7 @@ import robotfd_b200 as rfd  # noqa: E402
 CONFIG = 3          # uneven-batch generator (training and held-out pairs differ by seed)
 CHUNK = 4096        # pairs per labelling call
 TOL = 2.0 ** -33    # precise stop rule: ub - lb <= 2^-33 ub
+THRESHOLD_Y = float(np.log10(0.999 * TOL))  # y of the threshold probe
 DEFAULT_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bracket_model.npy")
 
 
@@ -43,9 +52,15 @@ def target(res):
 
 
 def pairs_of(npairs, seed, start, stop):
+    """Pairs start..stop-1 of the npairs-pair set (the generator runs in C, GIL released)."""
+    from concurrent.futures import ThreadPoolExecutor
     dims, n1, n2, styles, scales, noises = rfd.gen_batch_spec(CONFIG, npairs, seed)
-    return [rfd.gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]), float(scales[k]),
-                         float(noises[k]), seed, k) for k in range(start, stop)]
+
+    def one(k):
+        return rfd.gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]),
+                            float(scales[k]), float(noises[k]), seed, k)
+    with ThreadPoolExecutor(max(1, min(32, os.cpu_count() or 1))) as ex:
+        return list(ex.map(one, range(start, stop)))
 
 
 def label(ctx, npairs, seed, log=None):
@@ -88,10 +103,11 @@ def fold(params, mu, sd, ymu, ysd):
     return p.astype(np.float32)
 
 
-def train(X, y, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
-    """Trains a fresh network on (X, y); returns it with the normalisations folded in."""
+def train(X, y, epochs=150, batch=512, lr=2e-3, seed=0, device=0, log=None):
+    """Trains a fresh network on the pairs of (X, y) above the threshold; returns it with
+    the normalisations folded in, and the per-epoch loss."""
     import torch
-    ok = np.isfinite(y)
+    ok = np.isfinite(y) & (y > THRESHOLD_Y)
     X, y = X[ok], y[ok]
     mu = X.mean(0).astype(np.float64)
     sd = X.std(0).astype(np.float64)
@@ -105,6 +121,7 @@ def train(X, y, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
     model = rfd.Model(device, seed=seed)
     gen = torch.Generator(device=f"cuda:{device}").manual_seed(seed)
     n = len(y)
+    batch = min(batch, n)
     steps_per_epoch = max(1, n // batch)
     total = epochs * steps_per_epoch
     losses, step = [], 0
@@ -120,17 +137,18 @@ def train(X, y, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
             acc += model.train_step(xb.data_ptr(), yb.data_ptr(), len(idx), cur)
             step += 1
         losses.append(acc / steps_per_epoch * ysd)
-        if log:
+        if log and (ep + 1) % 10 == 0:
             log(f"epoch {ep + 1}/{epochs}: pinball loss {losses[-1]:.4f}")
     model.set_params(fold(model.get_params(), mu, sd, ymu, ysd))
     return model, losses
 
 
 def evaluate(ctx, model, npairs, seed, log=None):
-    """Held-out pairs solved with and without the network."""
-    stats = {"pairs": npairs, "plain_probes": 0, "learned_probes": 0, "plain_s": 0.0,
-             "learned_s": 0.0, "widened": 0, "one_probe": 0, "max_rel_dev": 0.0,
-             "max_rel_gap": 0.0}
+    """Held-out pairs solved plainly, with the network, and with the threshold probe alone."""
+    st = {k: 0 for k in ("plain_probes", "learned_probes", "tol_probes", "widened", "tol_widened",
+                         "one_probe", "plain_rounds", "learned_rounds", "tol_rounds", "tail",
+                         "tail_plain", "tail_learned", "tail_tol")}
+    st.update(plain_s=0.0, learned_s=0.0, tol_s=0.0, max_rel_dev=0.0, max_rel_gap=0.0)
     for s in range(0, npairs, CHUNK):
         e = min(npairs, s + CHUNK)
         pairs = pairs_of(npairs, seed, s, e)
@@ -141,31 +159,58 @@ def evaluate(ctx, model, npairs, seed, log=None):
         t1 = time.perf_counter()
         got = ctx.distance_batch(Ps, Qs, precise=True, model=model)
         t2 = time.perf_counter()
-        stats["plain_s"] += t1 - t0
-        stats["learned_s"] += t2 - t1
-        for a, b in zip(plain, got):
-            stats["plain_probes"] += a["probes"]
-            stats["learned_probes"] += b["probes"]
-            stats["widened"] += bool(b["flags"] & rfd.FLAG_BRACKET_WIDENED)
-            stats["one_probe"] += b["probes"] <= 1
+        # no network: a bracket at the VE-FD bound itself, i.e. the threshold probe and,
+        # when it fails, plain bisection above it
+        br = np.array([[r["vefd"] * (1 - 1e-15), r["vefd"]] for r in plain])
+        t3 = time.perf_counter()
+        tol_only = ctx.distance_batch(Ps, Qs, precise=True, brackets=br)
+        t4 = time.perf_counter()
+        st["plain_s"] += t1 - t0
+        st["learned_s"] += t2 - t1
+        st["tol_s"] += t4 - t3
+        st["plain_rounds"] += max(a["probes"] for a in plain)
+        st["learned_rounds"] += max(b["probes"] for b in got)
+        st["tol_rounds"] += max(c["probes"] for c in tol_only)
+        for a, b, c in zip(plain, got, tol_only):
+            st["plain_probes"] += a["probes"]
+            st["learned_probes"] += b["probes"]
+            st["tol_probes"] += c["probes"]
+            st["widened"] += bool(b["flags"] & rfd.FLAG_BRACKET_WIDENED)
+            st["tol_widened"] += bool(c["flags"] & rfd.FLAG_BRACKET_WIDENED)
+            st["one_probe"] += b["probes"] <= 1
+            if c["probes"] > 1:  # the threshold probe failed: a tail pair
+                st["tail"] += 1
+                st["tail_plain"] += a["probes"]
+                st["tail_learned"] += b["probes"]
+                st["tail_tol"] += c["probes"]
             if a["distance"] > 0:
-                stats["max_rel_dev"] = max(stats["max_rel_dev"],
-                                           abs(a["distance"] - b["distance"]) / a["distance"])
-                stats["max_rel_gap"] = max(stats["max_rel_gap"], (b["ub"] - b["lb"]) / b["ub"])
+                st["max_rel_dev"] = max(st["max_rel_dev"],
+                                        abs(a["distance"] - b["distance"]) / a["distance"])
+                st["max_rel_gap"] = max(st["max_rel_gap"], (b["ub"] - b["lb"]) / b["ub"])
         if log:
             log(f"evaluated {e}/{npairs} pairs")
     n = npairs
     return {
         "pairs": n,
-        "mean_probes_plain": stats["plain_probes"] / n,
-        "mean_probes_learned": stats["learned_probes"] / n,
-        "probes_saved_fraction": 1 - stats["learned_probes"] / max(stats["plain_probes"], 1),
-        "bracket_verification_failure_rate": stats["widened"] / n,
-        "one_probe_fraction": stats["one_probe"] / n,
-        "solves_per_s_plain": n / stats["plain_s"],
-        "solves_per_s_learned": n / stats["learned_s"],
-        "max_rel_deviation_from_plain": stats["max_rel_dev"],
-        "max_rel_final_gap": stats["max_rel_gap"],
+        "mean_probes_plain": st["plain_probes"] / n,
+        "mean_probes_learned": st["learned_probes"] / n,
+        "probes_saved_fraction": 1 - st["learned_probes"] / max(st["plain_probes"], 1),
+        "bracket_verification_failure_rate": st["widened"] / n,
+        "one_probe_fraction": st["one_probe"] / n,
+        "solves_per_s_plain": n / st["plain_s"],
+        "solves_per_s_learned": n / st["learned_s"],
+        "probe_rounds_plain": st["plain_rounds"],
+        "probe_rounds_learned": st["learned_rounds"],
+        "no_network_bracket": {
+            "mean_probes": st["tol_probes"] / n,
+            "failure_rate": st["tol_widened"] / n,
+            "probe_rounds": st["tol_rounds"],
+            "solves_per_s": n / st["tol_s"]},
+        "tail_pairs": st["tail"],
+        "tail_mean_probes": {k: st["tail_" + k] / max(st["tail"], 1)
+                             for k in ("plain", "learned", "tol")},
+        "max_rel_deviation_from_plain": st["max_rel_dev"],
+        "max_rel_final_gap": st["max_rel_gap"],
     }
 
 
@@ -175,16 +220,24 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--eval-pairs", type=int, default=4096)
     ap.add_argument("--eval-seed", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--eval-only", metavar="MODEL", help="evaluate saved parameters, no training")
     args = ap.parse_args(argv)
 
     def log(m):
         print(m, file=sys.stderr, flush=True)
 
     ctx = rfd.Context(args.device)
+    if args.eval_only:
+        model = rfd.Model.load(args.eval_only, device=args.device)
+        print(json.dumps({"eval": evaluate(ctx, model, args.eval_pairs, args.eval_seed, log),
+                          "model": args.eval_only}), flush=True)
+        model.close()
+        ctx.close()
+        return
     t0 = time.perf_counter()
     X, y, probes = label(ctx, args.pairs, args.seed, log)
     t_label = time.perf_counter() - t0
@@ -195,6 +248,7 @@ def main(argv=None):
     fin = y[np.isfinite(y)]
     out = {
         "train": {"pairs": args.pairs, "seed": args.seed, "usable": int(fin.size),
+                  "above_threshold": int(np.sum(fin > THRESHOLD_Y)),
                   "label_s": t_label, "train_s": t_train, "epochs": args.epochs,
                   "mean_plain_probes": float(probes.mean()),
                   "y_quantiles": {q: float(np.quantile(fin, q)) for q in (0.05, 0.5, 0.95, 0.99)},

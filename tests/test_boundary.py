@@ -169,6 +169,43 @@ def test_search_bracket_verification(built):
     assert st[0] <= fd <= st[1] and st[1] - st[0] <= 2.0 ** -33 * st[1]
 
 
+def run_search(built, st, ist, stop_mode, decide):
+    seq = []
+    more, e, st, ist = built.search_step(st, ist, stop_mode, False, 0.0, False)
+    while more:
+        seq.append(e)
+        more, e2, st, ist = built.search_step(st, ist, stop_mode, True, e, decide(e))
+        e = e2
+    return seq, st, ist
+
+
+@pytest.mark.parametrize("stop_mode,tol", [(0, np.finfo(np.float32).eps), (1, 2.0 ** -33)])
+def test_search_threshold_probe(built, stop_mode, tol):
+    """lb is proven: a bracket reaching below lb + tolerance probes that threshold first."""
+    lb = 0.7313
+    thr = lb + 0.999 * tol if stop_mode == 0 else lb * (1 + 0.999 * tol)
+    # distance within the tolerance of lb: one probe ends the search
+    fd = lb + 1e-3 * tol
+    seq, st, ist = run_search(built, [lb, 1.3, lb - 1e-3, lb + 1e-6 * tol, tol, 0.0], [1, 0, 64, 0],
+                              stop_mode, lambda e: e >= fd)
+    assert seq == [thr] and st[0] == lb and st[1] == thr and st[5] == thr
+    assert not (ist[3] & built.FLAG_BRACKET_WIDENED)
+    # distance far above: the threshold fails, the bracket below it is skipped, bisection
+    fd = lb + 0.01
+    seq, st, ist = run_search(built, [lb, 1.3, lb - 1e-3, lb + 1e-6 * tol, tol, 0.0], [1, 0, 64, 0],
+                              stop_mode, lambda e: e >= fd)
+    assert seq[0] == thr and seq[1] == (thr + 1.3) / 2
+    assert st[0] <= fd <= st[1] and not (ist[3] & built.FLAG_BRACKET_WIDENED)
+    # ... or a bracket above the threshold is verified after it
+    seq, st, ist = run_search(built, [lb, 1.3, lb - 1e-3, lb + 0.05, tol, 0.0], [1, 0, 64, 0],
+                              stop_mode, lambda e: e >= fd)
+    assert seq[:2] == [thr, lb + 0.05] and st[0] <= fd <= st[1]
+    # a bracket wholly above the threshold skips it
+    seq, st, ist = run_search(built, [0.7, 1.3, 0.72, 0.75, tol, 0.0], [1, 0, 64, 0], stop_mode,
+                              lambda e: e >= fd)
+    assert seq[0] == 0.75
+
+
 CPP_TEST = r'''
 #include <cstdio>
 #include "txtReader.hpp"

@@ -149,3 +149,25 @@ def test_gemm_matches_torch(built, torch, M, N, K, layout):
     got = dc.cpu().double()
     # FP32 accumulation of K products against float64
     assert float((got - want).abs().max()) <= 1e-5 * float(want.abs().max()) * max(1, K) ** 0.5
+
+
+def test_trained_network_saves_probes(ctx, built):
+    """The shipped network against the method without it, on held-out uneven-batch pairs."""
+    from robotfd_b200 import train_bracket
+    pairs = train_bracket.pairs_of(4096, 4, 0, 256)
+    Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+    plain = ctx.distance_batch(Ps, Qs, precise=True)
+    model = built.Model.pretrained(0)
+    got = ctx.distance_batch(Ps, Qs, precise=True, model=model)
+    tol = 2.0 ** -33
+    for a, b in zip(plain, got):
+        assert abs(a["distance"] - b["distance"]) <= 2 * tol * a["distance"]
+        assert b["lb"] <= b["distance"] <= b["ub"] and b["ub"] - b["lb"] <= tol * b["ub"]
+        assert b["flags"] & built.FLAG_BRACKET_USED
+    mean_plain = np.mean([a["probes"] for a in plain])
+    mean_learned = np.mean([b["probes"] for b in got])
+    assert mean_learned < 0.2 * mean_plain, (mean_plain, mean_learned)
+    # pairs the threshold probe does not end: the network's bracket against plain bisection
+    tail = [k for k, b in enumerate(got) if b["probes"] > 1]
+    if tail:
+        assert np.mean([got[k]["probes"] for k in tail]) < np.mean([plain[k]["probes"] for k in tail]) + 1
