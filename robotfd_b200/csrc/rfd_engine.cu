@@ -25,6 +25,7 @@
 
 #include "rfd.h"
 #include "rfd_device.cuh"
+#include "rfd_dfd.cuh"
 #include "rfd_team.cuh"
 #include "rfd_features.cuh"
 #include "rfd_mlp.h"
@@ -174,6 +175,46 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
       if (n == S - 1) {
         __threadfence();
         finalize<KIND>(st, pd, wa.active_pairs);
+        __threadfence();
+      }
+    }
+  }
+}
+
+// Dense DFD strips of 32*K rows (rfd_dfd.cuh), same in-order ticket scheme as wave_kernel
+// over the (pair, 32-row strip) item list: item (p, s) is strip s of 32*K rows, items past
+// the pair's last tall strip are skipped.
+template <int K>
+__global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
+  __shared__ double ring[kBlock / 32][3 * kDfdRing];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (bcast(lane == 0 ? ld_volatile(wa.active_pairs) : 0) == 0) return;
+  for (;;) {
+    unsigned t = 0;
+    int err = 0;
+    if (lane == 0) {
+      t = atomicAdd(wa.ticket, 1u);
+      err = ld_volatile(wa.error);
+    }
+    t = bcast(t);
+    if ((int)t >= wa.nitems || bcast(err)) return;
+    const int2 it = wa.items[t];
+    PairState* st = wa.st + it.x;
+    const int ok = lane == 0 ? (ld_volatile(&st->phase) == PH_DFD && ld_volatile(&st->active)) : 0;
+    if (!bcast(ok)) continue;
+    const PairDesc pd = wa.pairs[it.x];
+    const int S = (pd.n1 + 32 * K - 1) / (32 * K);
+    if (it.y >= S) continue;
+    const int status = pd.d == 2 ? dfd_strip<2, K>(wa, pd, st, it.y, ring[warp])
+                                 : dfd_strip<3, K>(wa, pd, st, it.y, ring[warp]);
+    if (status) return;
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      const int n = atomicAdd(&st->done_count, 1);
+      if (n == S - 1) {
+        __threadfence();
+        finalize<K_DFD>(st, pd, wa.active_pairs);
         __threadfence();
       }
     }
@@ -385,6 +426,8 @@ struct rfd_context {
   int grid[3] = {0, 0, 0};
   int team_grid[3] = {0, 0, 0};
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
+  int dfd_rows = 4;  // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
+  int dfd_grid = 0;
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
   size_t dws_size = 0;
@@ -664,7 +707,12 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (mode != MODE_DECIDE) {
     wa.phase = PH_DFD;
     wa.ticket = counters + li++;
-    wave_kernel<K_DFD><<<ctx->grid[K_DFD], kBlock, 0, st>>>(wa);
+    switch (ctx->dfd_rows) {
+      case 1: dfd_kernel<1><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
+      case 2: dfd_kernel<2><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
+      case 8: dfd_kernel<8><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
+      default: dfd_kernel<4><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
+    }
     RFD_CUDA(cudaGetLastError());
     if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
     for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
@@ -824,7 +872,6 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
   }
   c->num_sms = prop.multiProcessorCount;
   int occ[3] = {0, 0, 0};
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], wave_kernel<K_DFD>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], wave_kernel<K_VEFD>, kBlock, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], wave_kernel<K_DEC>, kBlock, 0);
   for (int k = 0; k < 3; ++k) c->grid[k] = std::max(1, occ[k]) * c->num_sms;
@@ -844,6 +891,17 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     c->team_grid[K_DEC] = std::max(1, o2) * c->num_sms;
     const char* e = getenv("RFD_SOLO");
     c->solo = e && e[0] == '1';
+    const char* dr = getenv("RFD_DFD_ROWS");
+    if (dr && (dr[0] == '1' || dr[0] == '2' || dr[0] == '4' || dr[0] == '8') && !dr[1])
+      c->dfd_rows = dr[0] - '0';
+    int od = 0;
+    switch (c->dfd_rows) {
+      case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1>, kBlock, 0); break;
+      case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2>, kBlock, 0); break;
+      case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8>, kBlock, 0); break;
+      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4>, kBlock, 0); break;
+    }
+    c->dfd_grid = std::max(1, od) * c->num_sms;
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
   }

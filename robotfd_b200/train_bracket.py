@@ -225,6 +225,10 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_OUT)
     ap.add_argument("--eval-only", metavar="MODEL", help="evaluate saved parameters, no training")
+    ap.add_argument("--save-dataset", metavar="NPZ", help="write the labelled pairs above the "
+                    "threshold (features, targets) and the set's statistics")
+    ap.add_argument("--dataset", metavar="NPZ", help="train on a file written by --save-dataset "
+                    "instead of labelling pairs")
     args = ap.parse_args(argv)
 
     def log(m):
@@ -239,19 +243,29 @@ def main(argv=None):
         ctx.close()
         return
     t0 = time.perf_counter()
-    X, y, probes = label(ctx, args.pairs, args.seed, log)
+    if args.dataset:
+        z = np.load(args.dataset)
+        X, y, probes = z["X"], z["y"], z["probes"]
+        stats = {k: float(z[k]) for k in ("usable", "mean_plain_probes")}
+    else:
+        X, y, probes = label(ctx, args.pairs, args.seed, log)
+        fin = y[np.isfinite(y)]
+        stats = {"usable": float(fin.size), "mean_plain_probes": float(probes.mean())}
+        keep = np.isfinite(y) & (y > THRESHOLD_Y)
+        X, y, probes = X[keep], y[keep], probes[keep]
+        if args.save_dataset:
+            np.savez(args.save_dataset, X=X, y=y, probes=probes, **stats)
     t_label = time.perf_counter() - t0
     t0 = time.perf_counter()
     model, losses = train(X, y, args.epochs, lr=args.lr, device=args.device, log=log)
     t_train = time.perf_counter() - t0
     model.save(args.out)
-    fin = y[np.isfinite(y)]
     out = {
-        "train": {"pairs": args.pairs, "seed": args.seed, "usable": int(fin.size),
-                  "above_threshold": int(np.sum(fin > THRESHOLD_Y)),
-                  "label_s": t_label, "train_s": t_train, "epochs": args.epochs,
-                  "mean_plain_probes": float(probes.mean()),
-                  "y_quantiles": {q: float(np.quantile(fin, q)) for q in (0.05, 0.5, 0.95, 0.99)},
+        "train": {"pairs": args.pairs, "seed": args.seed, "usable": int(stats["usable"]),
+                  "above_threshold": int(len(y)), "label_s": t_label, "train_s": t_train,
+                  "epochs": args.epochs, "lr": args.lr,
+                  "mean_plain_probes": stats["mean_plain_probes"],
+                  "y_quantiles_above": {q: float(np.quantile(y, q)) for q in (0.05, 0.5, 0.95)},
                   "loss_first": losses[0], "loss_last": losses[-1]},
         "eval": evaluate(ctx, model, args.eval_pairs, args.eval_seed, log),
         "out": os.path.relpath(args.out),

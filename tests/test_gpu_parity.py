@@ -175,3 +175,28 @@ def test_reference_driver_golden(ctx, built):
         r = ctx.distance(P, Q)
         assert r["endpoint"] == c["endpoint"], c["name"]
         assert r["distance"] == c["distance"], c["name"]
+
+
+@pytest.mark.parametrize("rows", ["1", "2", "4", "8"])
+def test_dfd_rows_per_lane_bitexact(built, rows):
+    """Dense DFD strips of 32 * rows rows: sizes around the strip and chunk boundaries."""
+    import os
+    old = os.environ.get("RFD_DFD_ROWS")
+    os.environ["RFD_DFD_ROWS"] = rows
+    try:
+        c = built.Context(0)
+    finally:
+        if old is None:
+            del os.environ["RFD_DFD_ROWS"]
+        else:
+            os.environ["RFD_DFD_ROWS"] = old
+    h = 32 * int(rows)
+    sizes = [(2, 2), (h - 1, 40), (h, 33), (h + 1, 65), (2 * h + 3, 31), (3 * h - 1, 257), (31, 2 * h)]
+    try:
+        for k, (n1, n2) in enumerate(sizes):
+            for d in (2, 3):
+                P, Q = walk_pair(k * 31 + n1 + d, n1, n2, d)
+                dfd, _ = c.bounds(P, Q, quirks=False)
+                assert dfd == np.sqrt(oracle.dfd_sq(P, Q)), (rows, n1, n2, d)
+    finally:
+        c.close()
