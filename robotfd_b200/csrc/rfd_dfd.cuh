@@ -2,42 +2,81 @@
 // src/intersection_algorithm_in_parallel.cu:435-641, cell recurrence :608-637).
 //
 // The DFD is a dense min-max DP with a cheap cell (one squared point distance), so its
-// sweep is bound by instruction issue and by the step-to-step latency of the skewed
-// wavefront, not by the geometry.  Compared with the generic strip (rfd_device.cuh):
-//   - a lane owns K consecutive rows, so a strip is 32*K rows high: per step a lane
-//     computes K cells in row order (each one's "from below" input is the previous row's
-//     carry of the same step), one shuffle brings the row below the lane's first row, and
-//     the strip-to-strip handoff (and its lag of two 32-column chunks) is paid once per
-//     32*K rows instead of once per 32;
-//   - the points of curve 2 a chunk of 32 steps needs are staged in a per-warp ring of 64
-//     columns in shared memory (structure of arrays, conflict-free), loaded into registers
-//     one chunk ahead, so no global load sits in a step;
+// sweep is bound by instruction issue and by how fast strips hand rows to each other, not
+// by the geometry.  Compared with the generic strip (rfd_device.cuh):
+//   - a lane owns K consecutive rows, in one of two layouts.  Skewed (for few, long pairs,
+//     where the sweep's latency decides): at step t, row k of lane l is at column
+//     t - (lK + k), so row k's "from below" input is row k-1's carry of the previous step
+//     and the K cells of a step are independent (ILP K); row k reuses the point row k-1
+//     used a step earlier, passed along in registers.  Stacked (for many pairs, where
+//     instruction throughput decides): the K rows are at the lane's column and computed in
+//     row order, fewer instructions per cell.  Either way a strip is 32K rows high, so K
+//     times fewer strips hand rows to each other;
+//   - the points of curve 2 a chunk of 32 steps needs are staged in a per-warp ring in
+//     shared memory (structure of arrays, conflict-free), loaded into registers one chunk
+//     ahead, so no global load sits in a step;
+//   - the row handed to the next strip carries its own validity: the rows are filled with
+//     an all-ones NaN pattern before the launch (dfd_fill_kernel), lane 31 stores each
+//     value of the strip's last row once as it is produced, and the next strip polls the
+//     values themselves, one 32-column chunk ahead of use.  A DFD value is never NaN (see
+//     dmin / dmax), and each word is written once, so no fence or progress word is needed
+//     and the load latency overlaps a chunk of steps;
+//   - min / max are compare-and-select: every value is a squared distance of finite points,
+//     0 or FLT_MAX, where they equal the reference's fmin / fmax (and a NaN coordinate
+//     cannot make a NaN value: a comparison with NaN selects the other operand);
 //   - there is no dead-region logic (the DFD is computed unpruned).
 // Boundary conditions of the reference (:614-626) are folded into the inputs: strip 0
 // reads the row above it as 0 at column 0 and FLT_MAX elsewhere, and every row reads
-// FLT_MAX to the left of column 0.  The operations of every cell, and their order, are
-// those of cell<K_DFD> in rfd_device.cuh, so results are bit-identical.
+// FLT_MAX to the left of column 0.  Every cell performs the operations of cell<K_DFD> in
+// rfd_device.cuh in the same order, so results are bit-identical.
 #pragma once
 
 #include "rfd_device.cuh"
 
 namespace rfd {
 
-constexpr int kDfdRing = 64;  // columns held per warp (two chunks)
+// Ring of curve-2 points per warp: at least 32K + 64 columns (a chunk ahead of the widest
+// span row 0 of the 32 lanes reads in one chunk, 31K + 32 columns).
+template <int K>
+struct DfdRing {
+  static constexpr int cols = K <= 2 ? 128 : (K <= 4 ? 256 : 512);
+  static_assert(cols >= 32 * K + 64, "ring too small");
+};
+constexpr unsigned long long kDfdEmpty = ~0ull;  // a NaN: "not yet written"
+
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
+
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
+// Relaxed (coherent, unordered) accesses of the handed-over row.  No ordering with other
+// memory accesses is needed, so there is no compiler memory barrier: the shared-memory
+// reads of the steps stay free to be scheduled around the stores.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
+}
 
 // Returns 0, or 1 on error / timeout (the error word is set).
-template <int D, int K>
+// SKEW: rows of a lane skewed by one column each (latency: independent cells per step), or
+// all at the lane's column (throughput: fewer instructions per cell, no point passing).
+template <int D, int K, bool SKEW>
 __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, const int s,
-                         double* ring /* [3][kDfdRing] per warp */) {
+                         double* ring /* [3][DfdRing<K>::cols] per warp */) {
+  constexpr int H = 32 * K;
+  constexpr int RC = DfdRing<K>::cols;
   const int lane = threadIdx.x & 31;
   const int R = pd.n1, C = pd.n2;
-  constexpr int H = 32 * K;
   const int S = (R + H - 1) / H;
-  const unsigned E = st->epoch;
   const bool has_prod = s > 0;
   const bool has_cons = s + 1 < S;
-  Prog* in_prog = has_prod ? pd.prog + (s - 1) : nullptr;
-  Prog* out_prog = has_cons ? pd.prog + s : nullptr;
   const double* in_bnd = has_prod ? pd.bnd + (size_t)(s - 1) * pd.cstride : nullptr;
   double* out_bnd = has_cons ? pd.bnd + (size_t)s * pd.cstride : nullptr;
 
@@ -45,6 +84,7 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   wt.start(wa, st, s);
 
   // rows of this lane (clamped loads beyond the last row: their values are never used)
+  const int base = SKEW ? lane * K : lane;  // row k of this lane is at column t - base - k*SKEW
   const int i0 = s * H + lane * K;
   double p[K][D];
 #pragma unroll
@@ -55,105 +95,129 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   }
   const int rlast = R - 1 - i0;  // index k of the pair's last row when this lane holds it
   const bool holds_last = s == S - 1 && rlast >= 0 && rlast < K;
+  // step at which that row reaches column C - 1
+  const int tres = C - 1 + base + (SKEW ? rlast : 0);
+  constexpr int kOutLag = SKEW ? H - 1 : 31;  // column of the last row = t - kOutLag
 
-  double bot[K];
+  double bot[K], carry[K], qp[K][D];
 #pragma unroll
-  for (int k = 0; k < K; ++k) bot[k] = kFltMax;
-  double carry = kFltMax;  // carry of this lane's last row (to the lane above)
-  double ob0 = kFltMax, ob1 = kFltMax;
+  for (int k = 0; k < K; ++k) {
+    bot[k] = kFltMax;
+    carry[k] = kFltMax;
+#pragma unroll
+    for (int e = 0; e < D; ++e) qp[k][e] = 0.0;
+  }
   double res = kFltMax;
-  int next_flush = 0;
-  const int nout = (C + 31) >> 5;
-  const int nsteps = C + 31;
+  const int nsteps = C + kOutLag;
   int status = 0;
 
-  auto flush = [&](int k) {
-    const int col = (k << 5) + lane;
-    const double v = (k & 1) ? ob1 : ob0;
-    if (col < C) __stcg(out_bnd + col, v);
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      st_release(&out_prog->word, ((unsigned long long)E << 32) | (unsigned)min((k + 1) << 5, C));
-    }
-  };
-  auto wait_cols = [&](unsigned need) -> int {
-    for (int it = 0;; ++it) {
-      const unsigned long long w = bcast(lane == 0 ? ld_acquire(&in_prog->word) : 0ull);
-      if ((unsigned)(w >> 32) == E && (unsigned)(w & 0xffffffffu) >= need) return 0;
-      const int r = wt.check(it);
-      if (r) return r;
-    }
-  };
   auto stage = [&](int c, const double (&q)[D]) {
-    const int slot = ((c << 5) + lane) & (kDfdRing - 1);
+    const int slot = ((c << 5) + lane) & (RC - 1);
 #pragma unroll
-    for (int e = 0; e < D; ++e) ring[e * kDfdRing + slot] = q[e];
+    for (int e = 0; e < D; ++e) ring[e * RC + slot] = q[e];
   };
   auto fetch = [&](int c, double (&q)[D]) {
     const int j = min((c << 5) + lane, C - 1);
 #pragma unroll
     for (int e = 0; e < D; ++e) q[e] = __ldg(pd.Q + (size_t)j * D + e);
   };
+  // the row above the strip at column 32c + lane (empty pattern while not yet written)
+  auto load_in = [&](int c) -> unsigned long long {
+    const int col = (c << 5) + lane;
+    if (!has_prod) return __double_as_longlong(col == 0 ? 0.0 : kFltMax);
+    if ((c << 5) >= C || col >= C) return __double_as_longlong(kFltMax);
+    return ld_relaxed_u64(in_bnd + col);
+  };
+  const bool store_out = has_cons && lane == 31;
+
+  // 32 steps of chunk c.  Column 0 (the reference's left boundary, FLT_MAX) only occurs in
+  // the first chunks (SKEW: K of them, else one), which alone carry that select.  The steps
+  // are unrolled by 8 only (those first chunks: not at all): with K rows, 2 and 3
+  // dimensions, a full unroll makes code that no longer fits the instruction cache, and
+  // fetch stalls then dominate.
+  auto steps = [&](const int c, const double inreg, auto first) {
+    constexpr bool FIRST = decltype(first)::value;
+    constexpr int kUnroll = FIRST ? 1 : 8;
+#pragma unroll kUnroll
+    for (int u = 0; u < 32; ++u) {
+      const int t = (c << 5) + u;
+      const double lin = __shfl_sync(kFull, inreg, u);
+      const double lup = __shfl_up_sync(kFull, carry[K - 1], 1);
+      const double left0 = lane == 0 ? lin : lup;
+      double q0[D];
+      const int slot = (t - base) & (RC - 1);
+#pragma unroll
+      for (int e = 0; e < D; ++e) q0[e] = ring[e * RC + slot];
+      if (SKEW) {
+        // rows in descending order: row k reads row k-1's values of the previous step
+#pragma unroll
+        for (int k = K - 1; k >= 0; --k) {
+          double q[D];
+#pragma unroll
+          for (int e = 0; e < D; ++e) q[e] = k == 0 ? q0[e] : qp[k - 1][e];
+          const double left = k == 0 ? left0 : carry[k - 1];
+          const double dist = dist_sq<D>(p[k], q);
+          const double b = (FIRST && t - base - k == 0) ? kFltMax : bot[k];
+          const double in = dmin(left, b);
+          const double top = dmax(dist, in);
+          carry[k] = dmin(top, b);
+          bot[k] = top;
+#pragma unroll
+          for (int e = 0; e < D; ++e) qp[k][e] = q[e];
+        }
+      } else {
+        // rows in ascending order at one column: each takes the row below's carry
+        double left = left0;
+        const bool j0 = FIRST && t - base == 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const double dist = dist_sq<D>(p[k], q0);
+          const double b = j0 ? kFltMax : bot[k];
+          const double in = dmin(left, b);
+          const double top = dmax(dist, in);
+          left = dmin(top, b);
+          bot[k] = top;
+        }
+        carry[K - 1] = left;
+      }
+      if (holds_last && t == tres) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (k == rlast) res = bot[k];
+      }
+      const int jo = t - kOutLag;  // column of the strip's last row at this step
+      if (store_out && jo >= 0 && jo < C) st_relaxed_f64(out_bnd + jo, carry[K - 1]);
+    }
+  };
 
   double qn[D];
   fetch(0, qn);
   stage(0, qn);
   __syncwarp();
+  unsigned long long nxt = load_in(0);
+  constexpr int kFirstChunks = SKEW ? K : 1;
 
   for (int c = 0; (c << 5) < nsteps; ++c) {
-    if (has_cons)
-      while (next_flush <= c - 2) flush(next_flush++);
-    // row above the strip for columns [32c, 32c + 32)
-    const int col = (c << 5) + lane;
-    double inreg = kFltMax;
-    if ((c << 5) < C) {
-      if (has_prod) {
-        const int r = wait_cols((unsigned)min((c + 1) << 5, C));
-        if (r) {  // 1 cannot happen (the DFD has no dead strips); 2: error
-          status = 1;
-          break;
-        }
-        if (col < C) inreg = __ldcg(in_bnd + col);
-      } else {
-        inreg = col == 0 ? 0.0 : kFltMax;
+    // wait until every column of this chunk's input row has been written
+    unsigned long long cur = nxt;
+    for (int it = 0;; ++it) {
+      if (__all_sync(kFull, cur != kDfdEmpty)) break;
+      const int r = wt.check(it);
+      if (r) {  // 1 cannot happen (the DFD has no dead strips); 2: error
+        status = 1;
+        break;
       }
+      if (cur == kDfdEmpty) cur = load_in(c);
     }
-    fetch(c + 1, qn);  // next chunk's points, in flight during this chunk
-#pragma unroll 4
-    for (int u = 0; u < 32; ++u) {
-      const int j = (c << 5) + u - lane;
-      const double lin = __shfl_sync(kFull, inreg, u);
-      const double lup = __shfl_up_sync(kFull, carry, 1);
-      double left = lane == 0 ? lin : lup;
-      const int slot = j & (kDfdRing - 1);
-      double q[D];
-#pragma unroll
-      for (int e = 0; e < D; ++e) q[e] = ring[e * kDfdRing + slot];
-      const bool j0 = j == 0;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const double dist = dist_sq<D>(p[k], q);
-        const double b = j0 ? kFltMax : bot[k];
-        const double in = fmin(left, b);
-        const double top = fmax(dist, in);
-        left = fmin(top, b);
-        bot[k] = top;
-        if (holds_last && k == rlast && j == C - 1) res = top;
-      }
-      carry = left;
-      const double o = __shfl_sync(kFull, carry, 31);
-      if (lane == ((u + 1) & 31)) {  // lane 31 produced column (c << 5) + u - 31
-        if (((((c << 5) + u - 31) >> 5) & 1) != 0) ob1 = o;
-        else ob0 = o;
-      }
-    }
+    if (status) break;
+    nxt = load_in(c + 1);  // in flight during this chunk
+    fetch(c + 1, qn);
+    if (c < kFirstChunks) steps(c, __longlong_as_double(cur), BoolC<true>{});
+    else steps(c, __longlong_as_double(cur), BoolC<false>{});
     __syncwarp();
     stage(c + 1, qn);
     __syncwarp();
   }
-  if (status == 0 && has_cons)
-    while (next_flush < nout) flush(next_flush++);
   if (holds_last) st->result = res;
   return status;
 }

@@ -181,12 +181,26 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
   }
 }
 
+// Marks the rows the DFD strips of 32*K rows hand to each other as not yet written (the
+// all-ones pattern, a NaN no DFD value takes).  One block per pair, grid-stride.
+__global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_strip) {
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    const PairDesc pd = pairs[p];
+    const long long S = (pd.n1 + rows_per_strip - 1) / rows_per_strip;
+    if (S < 2) continue;
+    // cstride is a multiple of 32 doubles and bnd 256-byte aligned: 16-byte stores
+    ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
+    const long long n = (S - 1) * pd.cstride / 2;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) b[k] = make_ulonglong2(kDfdEmpty, kDfdEmpty);
+  }
+}
+
 // Dense DFD strips of 32*K rows (rfd_dfd.cuh), same in-order ticket scheme as wave_kernel
 // over the (pair, 32-row strip) item list: item (p, s) is strip s of 32*K rows, items past
 // the pair's last tall strip are skipped.
-template <int K>
+template <int K, bool SKEW>
 __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
-  __shared__ double ring[kBlock / 32][3 * kDfdRing];
+  __shared__ double ring[kBlock / 32][3 * DfdRing<K>::cols];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (bcast(lane == 0 ? ld_volatile(wa.active_pairs) : 0) == 0) return;
   for (;;) {
@@ -205,8 +219,8 @@ __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
     const PairDesc pd = wa.pairs[it.x];
     const int S = (pd.n1 + 32 * K - 1) / (32 * K);
     if (it.y >= S) continue;
-    const int status = pd.d == 2 ? dfd_strip<2, K>(wa, pd, st, it.y, ring[warp])
-                                 : dfd_strip<3, K>(wa, pd, st, it.y, ring[warp]);
+    const int status = pd.d == 2 ? dfd_strip<2, K, SKEW>(wa, pd, st, it.y, ring[warp])
+                                 : dfd_strip<3, K, SKEW>(wa, pd, st, it.y, ring[warp]);
     if (status) return;
     __syncwarp();
     if (lane == 0) {
@@ -426,8 +440,9 @@ struct rfd_context {
   int grid[3] = {0, 0, 0};
   int team_grid[3] = {0, 0, 0};
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
-  int dfd_rows = 4;  // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
-  int dfd_grid = 0;
+  int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
+  int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
+  int dfd_grid[2] = {0, 0};  // [stacked, skewed]
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
   size_t dws_size = 0;
@@ -707,11 +722,27 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (mode != MODE_DECIDE) {
     wa.phase = PH_DFD;
     wa.ticket = counters + li++;
-    switch (ctx->dfd_rows) {
-      case 1: dfd_kernel<1><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
-      case 2: dfd_kernel<2><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
-      case 8: dfd_kernel<8><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
-      default: dfd_kernel<4><<<ctx->dfd_grid, kBlock, 0, st>>>(wa); break;
+    dfd_fill_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(
+        dd, (int)npairs, 32 * ctx->dfd_rows);
+    ++launches;
+    {
+      // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
+      // latency decides), stacked rows otherwise (instruction throughput decides)
+      int64_t strips = 0;
+      for (int64_t p = 0; p < npairs; ++p) strips += (n1s[p] + 32 * ctx->dfd_rows - 1) / (32 * ctx->dfd_rows);
+      const int sk = ctx->dfd_skew >= 0 ? ctx->dfd_skew
+                                         : (strips < 2 * (int64_t)ctx->dfd_grid[1] * (kBlock / 32) ? 1 : 0);
+      const int g = ctx->dfd_grid[sk];
+      switch (ctx->dfd_rows * 2 + sk) {
+        case 2: dfd_kernel<1, false><<<g, kBlock, 0, st>>>(wa); break;
+        case 3: dfd_kernel<1, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 4: dfd_kernel<2, false><<<g, kBlock, 0, st>>>(wa); break;
+        case 5: dfd_kernel<2, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 8: dfd_kernel<4, false><<<g, kBlock, 0, st>>>(wa); break;
+        case 9: dfd_kernel<4, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 16: dfd_kernel<8, false><<<g, kBlock, 0, st>>>(wa); break;
+        default: dfd_kernel<8, true><<<g, kBlock, 0, st>>>(wa); break;
+      }
     }
     RFD_CUDA(cudaGetLastError());
     if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
@@ -894,14 +925,22 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     const char* dr = getenv("RFD_DFD_ROWS");
     if (dr && (dr[0] == '1' || dr[0] == '2' || dr[0] == '4' || dr[0] == '8') && !dr[1])
       c->dfd_rows = dr[0] - '0';
-    int od = 0;
-    switch (c->dfd_rows) {
-      case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1>, kBlock, 0); break;
-      case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2>, kBlock, 0); break;
-      case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8>, kBlock, 0); break;
-      default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4>, kBlock, 0); break;
+    const char* dk = getenv("RFD_DFD_SKEW");
+    if (dk && (dk[0] == '0' || dk[0] == '1') && !dk[1]) c->dfd_skew = dk[0] - '0';
+    for (int sk = 0; sk < 2; ++sk) {
+      int od = 0;
+      switch (c->dfd_rows * 2 + sk) {
+        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, false>, kBlock, 0); break;
+        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, true>, kBlock, 0); break;
+        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, false>, kBlock, 0); break;
+        case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, true>, kBlock, 0); break;
+        case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, false>, kBlock, 0); break;
+        case 9: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, true>, kBlock, 0); break;
+        case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, false>, kBlock, 0); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, true>, kBlock, 0); break;
+      }
+      c->dfd_grid[sk] = std::max(1, od) * c->num_sms;
     }
-    c->dfd_grid = std::max(1, od) * c->num_sms;
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
   }

@@ -177,19 +177,23 @@ def test_reference_driver_golden(ctx, built):
         assert r["distance"] == c["distance"], c["name"]
 
 
+@pytest.mark.parametrize("skew", ["0", "1"])
 @pytest.mark.parametrize("rows", ["1", "2", "4", "8"])
-def test_dfd_rows_per_lane_bitexact(built, rows):
-    """Dense DFD strips of 32 * rows rows: sizes around the strip and chunk boundaries."""
+def test_dfd_rows_per_lane_bitexact(built, rows, skew):
+    """Dense DFD strips of 32 * rows rows, stacked or skewed rows per lane: sizes around the
+    strip and chunk boundaries."""
     import os
-    old = os.environ.get("RFD_DFD_ROWS")
-    os.environ["RFD_DFD_ROWS"] = rows
+    env = {"RFD_DFD_ROWS": rows, "RFD_DFD_SKEW": skew}
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
     try:
         c = built.Context(0)
     finally:
-        if old is None:
-            del os.environ["RFD_DFD_ROWS"]
-        else:
-            os.environ["RFD_DFD_ROWS"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
     h = 32 * int(rows)
     sizes = [(2, 2), (h - 1, 40), (h, 33), (h + 1, 65), (2 * h + 3, 31), (3 * h - 1, 257), (31, 2 * h)]
     try:
@@ -197,6 +201,6 @@ def test_dfd_rows_per_lane_bitexact(built, rows):
             for d in (2, 3):
                 P, Q = walk_pair(k * 31 + n1 + d, n1, n2, d)
                 dfd, _ = c.bounds(P, Q, quirks=False)
-                assert dfd == np.sqrt(oracle.dfd_sq(P, Q)), (rows, n1, n2, d)
+                assert dfd == np.sqrt(oracle.dfd_sq(P, Q)), (rows, skew, n1, n2, d)
     finally:
         c.close()
