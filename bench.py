@@ -1,19 +1,23 @@
 #!/usr/bin/env python
 """Benchmark of the continuous Frechet distance engine on B200.
 
-One step is one full solve (endpoint bound, DFD, VE-FD, epsilon search to 2^-33 relative,
-i.e. within 1e-9 of the FP64 result) of the long-pair workload: two 200,000-point 3D
-robot-like paths (Catmull-Rom through 2,000 waypoints U[-100,100]^3, the second path under
-a 20-knot monotone time warp plus N(0, 0.1^2) noise, seed 1), 4.0e10 free-space cells per
-decision.  Inputs are synthetic and seeded (the reference ships no data).
+One step is one full solve (endpoint bound, DFD, VE-FD, learned bracket, epsilon search to
+2^-33 relative, i.e. within 1e-9 of the FP64 result) of the long-pair workload: two
+200,000-point 3D robot-like paths (Catmull-Rom through 2,000 waypoints U[-100,100]^3, the
+second path under a 20-knot monotone time warp plus N(0, 0.1^2) noise, seed 1), 4.0e10
+free-space cells per decision.  Inputs are synthetic and seeded (the reference ships no data).
 
-  value : FD solves/s with both curves resident in HBM (rfd_distance on device pointers)
+  value : FD solves/s with both curves resident in HBM (rfd_distance on device pointers, the
+          shipped bracket network)
   e2e   : the same through the C ABI with host buffers (H2D copy, solve, D2H result)
+  plain : the plain method (bisection of [VE-FD, DFD], no bracket) on the same pair
+  batch : the 4096-pair uneven batch (lognormal lengths, seed 2): learned and plain batched
+          calls, and single-pair plain calls on a sample of it
   roofline : the dominant phase kernel against the measured FP64 FMA peak
   cpu_baseline : the CPU oracle (dense FP64 restatement, OpenMP) on a bounded sample,
-                 extrapolated to the full pair
+                 extrapolated to the plain method's probes on the full pair
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-batch]
 Under torchrun every rank solves the same pair (the path does not shard: replicas only).
 """
 import argparse
@@ -36,7 +40,8 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
 DEC_DRAM_BYTES_20K = 2.408192e6
-KERNEL_OF_PHASE = {"dfd": "wave_kernel<K_DFD>", "vefd": "team_kernel<K_VEFD>",
+DFD_DRAM_BYTES_200K = 1.10e9 + 1.20e9
+KERNEL_OF_PHASE = {"dfd": "dfd_kernel<8>", "vefd": "team_kernel<K_VEFD>",
                    "search": "team_kernel<K_DEC>"}
 FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3, "vefd": lambda d: 24 * d + 2,
                   "search": lambda d: 12 * d + 22}
@@ -52,6 +57,11 @@ def parse():
                     help="points per curve of the CPU-baseline sample")
     ap.add_argument("--points", type=int, default=200000,
                     help="points per curve of the long pair (smaller values: profiling cases)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 4096-pair batch leg")
+    ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-method solves")
+    ap.add_argument("--profile-batch", type=int, default=0, metavar="N",
+                    help="profiling case: one batched call (one probe) on the first N pairs of "
+                         "the uneven batch, then exit (no JSON line)")
     return ap.parse_args()
 
 
@@ -175,12 +185,65 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_pairs(npairs=4096, seed=2):
+    """The uneven batch (config 2 generator), generated on all host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    import robotfd_b200 as rfd
+    dims, n1, n2, styles, scales, noises = rfd.gen_batch_spec(2, npairs, seed)
+
+    def one(k):
+        return rfd.gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]),
+                            float(scales[k]), float(noises[k]), seed, k)
+    with ThreadPoolExecutor(max(1, min(32, os.cpu_count() or 1))) as ex:
+        return list(ex.map(one, range(npairs)))
+
+
+def batch_leg(ctx, model, timed, sample=128):
+    """4096 uneven pairs: learned batched, plain batched, and plain single-pair calls on a
+    fixed sample (every 32nd pair), each timed with CUDA events on the context stream."""
+    pairs = batch_pairs()
+    Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+    n = len(Ps)
+    ctx.distance_batch(Ps[:64], Qs[:64], precise=True, model=model)  # warm
+    t_l, learned = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model), 2)
+    t_p, plain = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True), 1)
+    idx = list(range(0, n, max(1, n // sample)))[:sample]
+    t_s, single = timed(lambda: [ctx.distance(Ps[k], Qs[k], precise=True) for k in idx], 1)
+    dev = max(abs(a["distance"] - b["distance"]) / a["distance"]
+              for a, b in zip(plain, learned) if a["distance"] > 0)
+    assert dev <= 1e-9, f"learned and plain batch results differ by {dev:.3g}"
+    for k, r in zip(idx, single):
+        assert r["distance"] == plain[k]["distance"], "single and batched plain results differ"
+    sps = {"learned_batched": n / (statistics.median(t_l) * 1e-3),
+           "plain_batched": n / (statistics.median(t_p) * 1e-3),
+           "plain_single_calls": len(idx) / (sum(t_s) * 1e-3)}
+    return {
+        "workload": "4096 uneven pairs (2D/3D 50/50, lognormal lengths median 2000, sigma 1, "
+                    "clipped [100, 50000], walk/spline shapes, seed 2); FD to 2^-33 relative",
+        "solves_per_s": sps,
+        "learned_batched_vs_plain_single_calls": sps["learned_batched"] / sps["plain_single_calls"],
+        "plain_single_sample": f"{len(idx)} pairs (every {n // len(idx)}th), one call each",
+        "mean_probes": {"learned": statistics.mean(r["probes"] for r in learned),
+                        "plain": statistics.mean(r["probes"] for r in plain)},
+        "probe_rounds": {"learned": max(r["probes"] for r in learned),
+                         "plain": max(r["probes"] for r in plain)},
+        "max_rel_dev_learned_vs_plain": dev,
+        "cells": sum(len(p) * len(q) for p, q in pairs),
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
     import torch
     import robotfd_b200 as rfd
+    if args.profile_batch:
+        pairs = batch_pairs()[: args.profile_batch]
+        ctx = rfd.Context(0)
+        ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True, max_probes=1)
+        ctx.close()
+        return
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -192,19 +255,25 @@ def main():
     ctx = rfd.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    model = rfd.Model.pretrained(local)
     P, Q = workload(args.points)
     n1, n2, d = len(P), len(Q), P.shape[1]
     dP = torch.from_numpy(P).cuda()
     dQ = torch.from_numpy(Q).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    torch.cuda.synchronize()
 
     def step_dev():
-        return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True)
+        return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True,
+                                   model=model)
 
     def step_host():
-        return ctx.distance(P, Q, precise=True)
+        return ctx.distance(P, Q, precise=True, model=model)
 
-    def timed(fn, k, tag):
+    def step_plain():
+        return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True)
+
+    def timed(fn, k):
         times, res = [], None
         for _ in range(k):
             flush.fill_(1)  # L2 flush outside the event pair
@@ -226,7 +295,7 @@ def main():
     clocks = Clocks(local)
     clocks.start()
     torch.cuda.synchronize()
-    times, res = timed(step_dev, args.steps, "value")
+    times, res = timed(step_dev, args.steps)
     torch.cuda.synchronize()
     clk = clocks.stop()
     phases = ctx.phase_times(enable=0)
@@ -239,9 +308,11 @@ def main():
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
 
-    # e2e: host buffers through the C ABI, copies inside the timed region
+    # e2e: host buffers through the C ABI, copies inside the timed region (one untimed call
+    # first: host inputs add the curves to the device workspace, which may then grow)
+    step_host()
     ctx.phase_times(enable=1)
-    etimes, eres = timed(step_host, args.steps, "e2e")
+    etimes, eres = timed(step_host, args.steps)
     ephase = ctx.phase_times(enable=0)
     e_ms = sum(etimes)
     if dist:
@@ -250,6 +321,14 @@ def main():
         e_ms = float(t.item())
     e2e_value = world * args.steps / (e_ms / 1e3)
     assert eres["distance"] == res["distance"], "host and device inputs disagree"
+
+    # the plain method on the same pair (no bracket): the reference's probe sequence
+    step_plain()
+    ctx.phase_times(enable=1)
+    ptimes, pres = timed(step_plain, args.plain_steps)
+    pphase = ctx.phase_times(enable=0)
+    rel = abs(pres["distance"] - res["distance"]) / pres["distance"]
+    assert rel <= 1e-9, f"learned and plain results differ by {rel:.3g}"
 
     peak = ctx.fp64_peak()
     calls = max(phases["calls"], 1)
@@ -268,7 +347,13 @@ def main():
         # 20,000-point case (cold cache: every touched point record and boundary word once);
         # the touched data grows with the points, not the cells, so it scales by n1 + n2
         traffic = DEC_DRAM_BYTES_20K * (n1 + n2) / 40000
+    elif dom == "dfd":
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum of the DFD launch on the full
+        # 200,000-point pair (one pass): the boundary rows the 256-row strips hand over,
+        # scaled by their count for other sizes
+        traffic = DFD_DRAM_BYTES_200K * ((n1 + 255) // 256 - 1) * n2 / (781 * 200000)
     sm_mhz = clk.get("sm_mhz") or 1965.0
+    pcalls = max(pphase["calls"], 1)
 
     line = {
         "metric": METRIC,
@@ -284,11 +369,18 @@ def main():
         "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD if args.points == 200000 else
-                   f"long-pair generator at {args.points} points per curve", "n1": n1, "n2": n2, "dims": d,
-                   "stop": "ub-lb <= 2^-33 ub", "parallelism": f"replicas x{world}",
+                   f"long-pair generator at {args.points} points per curve", "n1": n1, "n2": n2,
+                   "dims": d, "stop": "ub-lb <= 2^-33 ub", "form": "learned bracket (shipped network)",
+                   "parallelism": f"replicas x{world}",
                    "l2": "flushed before every step (256 MiB write outside the timed events)"},
         "fd": res["distance"],
+        "dfd": res["dfd"],
+        "vefd": res["vefd"],
         "probes": res["probes"],
+        "plain": {"solves_per_s": args.plain_steps / (sum(ptimes) * 1e-3),
+                  "ms_per_solve": sum(ptimes) / args.plain_steps, "probes": pres["probes"],
+                  "phase_ms": {k: pphase[k + "_ms"] / pcalls for k in ("dfd", "vefd", "search")},
+                  "rel_dev_vs_learned": rel},
         "free_space_cells_per_s": {
             "nominal": res["cells_nominal"] / (ph_ms["search"] * 1e-3),
             "evaluated": res["cells_evaluated"] / (ph_ms["search"] * 1e-3),
@@ -303,28 +395,33 @@ def main():
                      "traffic": traffic,
                      "peak_source": "measured FP64 FMA throughput (rfd_fp64_peak), this GPU",
                      "flops_per_cell": FLOPS_PER_CELL[dom](d), "cells": cells[dom],
-                     "traffic_note": "bytes per launch, ncu cold-cache capture at 20k points "
-                                     "scaled by points"},
-        # the decision is bound by its dependency chain, not by flops or bytes: the wavefront
-        # has n1 + n2 anti-diagonals, so this is the latency each one adds to a probe
+                     "traffic_note": ("bytes per launch, ncu capture of the full-size launch"
+                                      if dom == "dfd" else
+                                      "bytes per launch, ncu cold-cache capture at 20k points "
+                                      "scaled by points")},
+        # the pruned sweeps are bound by their dependency chain, not by flops or bytes: the
+        # wavefront has n1 + n2 anti-diagonals, so this is the latency each one adds
         "critical_path": {
             "antidiagonals": n1 + n2,
-            "ms_per_probe": ph_ms["search"] / max(res["probes"], 1),
-            "cycles_per_antidiagonal": ph_ms["search"] / max(res["probes"], 1) * 1e-3
-                                       * sm_mhz * 1e6 / (n1 + n2)},
+            "ms_per_probe": pphase["search_ms"] / pcalls / max(pres["probes"], 1),
+            "cycles_per_antidiagonal": pphase["search_ms"] / pcalls / max(pres["probes"], 1)
+                                       * 1e-3 * sm_mhz * 1e6 / (n1 + n2)},
         "e2e": {"value": e2e_value, "unit": "solves/s",
                 "h2d_bytes_per_step": ephase["h2d_bytes"] / max(ephase["calls"], 1),
                 "d2h_bytes_per_step": ephase["d2h_bytes"] / max(ephase["calls"], 1)},
         "gpu_launches": int(phases["launches"]),
         "clocks": clk,
     }
+    if not args.no_batch:
+        line["batch"] = batch_leg(ctx, model, timed)
     if rank == 0:
         if world == 1:
-            line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, res["probes"])
+            line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, pres["probes"])
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    model.close()
     ctx.close()
 
 

@@ -182,16 +182,19 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
 }
 
 // Marks the rows the DFD strips of 32*K rows hand to each other as not yet written (the
-// all-ones pattern, a NaN no DFD value takes).  One block per pair, grid-stride.
+// all-ones pattern, a NaN no DFD value takes).  Pairs are spread over grid rows (y) and
+// each pair's rows over grid columns (x), so one large pair uses every SM.
 __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_strip) {
-  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int p = blockIdx.y; p < npairs; p += gridDim.y) {
     const PairDesc pd = pairs[p];
     const long long S = (pd.n1 + rows_per_strip - 1) / rows_per_strip;
     if (S < 2) continue;
     // cstride is a multiple of 32 doubles and bnd 256-byte aligned: 16-byte stores
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
     const long long n = (S - 1) * pd.cstride / 2;
-    for (long long k = threadIdx.x; k < n; k += blockDim.x) b[k] = make_ulonglong2(kDfdEmpty, kDfdEmpty);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+      b[k] = make_ulonglong2(kDfdEmpty, kDfdEmpty);
   }
 }
 
@@ -722,8 +725,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (mode != MODE_DECIDE) {
     wa.phase = PH_DFD;
     wa.ticket = counters + li++;
-    dfd_fill_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(
-        dd, (int)npairs, 32 * ctx->dfd_rows);
+    {
+      const int gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
+      const int gx = std::max(1, 8 * ctx->num_sms / gy);
+      dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(dd, (int)npairs, 32 * ctx->dfd_rows);
+    }
     ++launches;
     {
       // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
