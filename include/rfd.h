@@ -83,7 +83,8 @@ typedef struct rfd_result {
   double endpoint;          /* max(|p0 - q0|, |pn - qm|) (src/frechet.cpp:30) */
   double lb, ub;            /* final bracket */
   int64_t cells_nominal;    /* sum over decisions of (n1-1)(n2-1) */
-  int64_t cells_evaluated;  /* decision cells the kernels actually evaluated */
+  int64_t cells_evaluated;  /* decision cells the kernels actually evaluated (includes
+                               speculative tiles, so it varies slightly from run to run) */
   int64_t cells_fp64;       /* of those, cells whose intervals were computed in FP64 */
   int64_t cells_vefd;       /* VE-FD cells evaluated (of (n1-1)(n2-1) per pass) */
   int32_t probes;           /* decisions made */
@@ -211,6 +212,14 @@ int32_t rfd_gen_pair(int32_t style, int32_t dims, int64_t n1, int64_t n2, double
                      int64_t* out_n2);
 int32_t rfd_gen_batch_spec(int32_t config, int64_t npairs, uint64_t seed, int32_t* dims, int64_t* n1s,
                            int64_t* n2s, int32_t* styles, double* scales, double* noises);
+
+/* ---- FP32 filter of the free intervals (host-callable copy of the device logic, for
+   tests; no reference counterpart) ----
+   cls[e] = 1 when the FP64 free interval of the edge a_e -> b_e (di = b - a in FP64) around
+   x_e at radius^2 r2 is certainly empty, 2 when it is certainly (0, 1), 0 when it has to be
+   computed in FP64.  Arrays are [n][dims]; A[e] = |b_e - a_e|^2 as the engine computes it. */
+int32_t rfd_interval_class(int64_t n, const double* x, const double* a, const double* b,
+                           const double* A, double r2, int32_t dims, int32_t* cls);
 
 /* ---- search state machine (host-callable copy of the device logic, for tests) ----
    Applies one decision outcome to a bracket search and proposes the next probe.

@@ -48,6 +48,8 @@ def lib():
                                         ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_int, _dp, _ip]
         L.rfd_oracle_max_threads.restype = ctypes.c_int
+        L.rfd_oracle_free_intervals.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                                ctypes.c_int, _dp, _dp]
         _LIB = L
     return _LIB
 
@@ -142,3 +144,17 @@ def search(P, Q, lb, ub, stop_mode=0, tol=None, max_probes=200, threads=1):
     if rc:
         raise RuntimeError(f"oracle search failed ({rc})")
     return out[0], out[1], out[2], probes.value
+
+
+def free_intervals(x, a, b, A, r2):
+    """FP64 free intervals of the edges a_e -> b_e around x_e (arrays [n][d]; A [n])."""
+    x, a, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, a, b))
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    inv2A = 0.5 / A
+    n, d = x.shape
+    lo, hi = np.empty(n), np.empty(n)
+    rc = lib().rfd_oracle_free_intervals(n, _ptr(x), _ptr(a), _ptr(b), _ptr(A), _ptr(inv2A),
+                                         float(r2), d, _ptr(lo), _ptr(hi))
+    if rc:
+        raise RuntimeError("oracle free_intervals failed")
+    return lo, hi

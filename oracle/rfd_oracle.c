@@ -387,6 +387,17 @@ int rfd_oracle_search(const double* P, int64_t n1, const double* Q, int64_t n2, 
   return 0;
 }
 
+/* Free intervals of n edges (test entry): edge e is the segment a_e -> b_e against the ball
+   of radius^2 r2 around x_e, with A_e = |b_e - a_e|^2 and inv2A_e = 0.5 / A_e as given. */
+int rfd_oracle_free_intervals(int64_t n, const double* x, const double* a, const double* b,
+                              const double* A, const double* inv2A, double r2, int d, double* lo,
+                              double* hi) {
+  if (n < 0 || (d != 2 && d != 3)) return 1;
+  for (int64_t e = 0; e < n; ++e)
+    free_interval(x + e * d, a + e * d, b + e * d, A[e], inv2A[e], r2, d, lo + e, hi + e);
+  return 0;
+}
+
 int rfd_oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -54,7 +54,7 @@ EXPORTS = (
     "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
     "rfd_model_num_params", "rfd_model_create", "rfd_model_destroy", "rfd_model_set_params",
     "rfd_model_get_params", "rfd_model_forward", "rfd_model_gradients", "rfd_model_train_step",
-    "rfd_features", "rfd_gemm_bf16",
+    "rfd_features", "rfd_gemm_bf16", "rfd_interval_class",
 )
 
 
@@ -155,6 +155,8 @@ def lib():
     L.rfd_gen_batch_spec.restype = i32
     L.rfd_search_step.argtypes = [_dp, _i32p, i32, i32, dbl, i32, _dp]
     L.rfd_search_step.restype = i32
+    L.rfd_interval_class.argtypes = [i64, _dp, _dp, _dp, _dp, dbl, i32, _i32p]
+    L.rfd_interval_class.restype = i32
     L.rfd_decide_noalloc.argtypes = [vp, i64, vp, i64, i32, dbl, vp, vp]
     L.rfd_decide_noalloc.restype = i32
     fp = ctypes.POINTER(ctypes.c_float)
@@ -430,6 +432,19 @@ def search_step(state, istate, stop_mode, have_outcome, eps, reachable):
     more = lib().rfd_search_step(st, ist, stop_mode, int(bool(have_outcome)), float(eps),
                                  int(bool(reachable)), ctypes.byref(nxt))
     return bool(more), nxt.value, list(st), list(ist)
+
+
+def interval_class(x, a, b, A, r2):
+    """Host copy of the FP32 filter: per edge a_e -> b_e around x_e, 1 = certainly empty,
+    2 = certainly (0, 1), 0 = computed in FP64 (rfd_interval_class)."""
+    x, a, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, a, b))
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n, d = x.shape
+    cls = np.empty(n, dtype=np.int32)
+    _check(lib().rfd_interval_class(n, x.ctypes.data_as(_dp), a.ctypes.data_as(_dp),
+                                    b.ctypes.data_as(_dp), A.ctypes.data_as(_dp), float(r2), d,
+                                    cls.ctypes.data_as(_i32p)))
+    return cls
 
 
 def decide_noalloc(p_dev, n1, q_dev, n2, dims, radius, stream, out_dev):

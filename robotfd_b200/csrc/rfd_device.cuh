@@ -76,7 +76,8 @@ struct PairState {
   int phase, active, quirks, dense, decide_only, flags;
   int dead_from, done_count;
   int use_model;
-  int pad[2];
+  int filter;  // 1: decision intervals through the FP32 filter (RFD_PREC_FP32_FILTER)
+  int pad;
 };
 
 template <int D>

@@ -26,6 +26,7 @@
 #include "rfd.h"
 #include "rfd_device.cuh"
 #include "rfd_dfd.cuh"
+#include "rfd_filter.h"
 #include "rfd_team.cuh"
 #include "rfd_features.cuh"
 #include "rfd_mlp.h"
@@ -277,6 +278,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       sh->go = go;
       sh->quit = quit;
       sh->evaluated = 0ull;
+      sh->evaluated64 = 0ull;
       sh->status = 0;
     }
     __syncthreads();
@@ -299,6 +301,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       const int S = (pd.n1 - 1 + 31) >> 5;
       const unsigned long long ev = sh->evaluated;
       if (ev) atomicAdd(KIND == K_DEC ? &st->cells_eval : &st->cells_vefd, ev);
+      if (KIND == K_DEC && sh->evaluated64) atomicAdd(&st->cells_fp64, sh->evaluated64);
       __threadfence();
       const int n = atomicAdd(&st->done_count, 1);
       if (n == S - 1) {
@@ -529,6 +532,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (o.max_probes < 0 || o.max_probes > RFD_MAX_PROBES) return fail(RFD_ERR_ARG, "max_probes");
   if (o.stop_mode != RFD_STOP_ABS && o.stop_mode != RFD_STOP_REL) return fail(RFD_ERR_ARG, "stop_mode");
   if (!(o.tol >= 0.0)) return fail(RFD_ERR_ARG, "tol");
+  if (o.precision != RFD_PREC_FP64 && o.precision != RFD_PREC_FP32_FILTER)
+    return fail(RFD_ERR_ARG, "precision");
   for (int64_t p = 0; p < npairs; ++p) {
     int rc = check_pair(c1s[p], n1s[p], c2s[p], n2s[p], dims[p]);
     if (rc) return rc;
@@ -655,6 +660,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     s.quirks = o.reference_quirks;
     s.dense = o.dense;
     s.use_model = use_model ? 1 : 0;
+    s.filter = o.precision == RFD_PREC_FP32_FILTER ? 1 : 0;
     s.blo = s.bhi = NAN;
     if (o.bracket && mode == MODE_DISTANCE) {
       s.blo = o.bracket[2 * p];
@@ -838,7 +844,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     r.flags = s.flags | s.srch.flags;
     r.cells_nominal = (int64_t)s.cells_nominal;
     r.cells_evaluated = (int64_t)s.cells_eval;
-    r.cells_fp64 = (int64_t)s.cells_eval;
+    r.cells_fp64 = (int64_t)(s.filter ? s.cells_fp64 : s.cells_eval);
     r.cells_vefd = (int64_t)s.cells_vefd;
     if (mode == MODE_DECIDE) r.distance = s.result;  // propagated right UB of the last cell
     if (mode == MODE_DISTANCE && s.phase != PH_DONE)
@@ -1126,6 +1132,19 @@ int32_t rfd_features(rfd_context* ctx, int64_t npairs, const double* const* c1s,
   RFD_CUDA(cudaMemcpyAsync(out, base + o_feat, sizeof(float) * rfd_mlp::kInputWidth * npairs,
                            cudaMemcpyDeviceToHost, st));
   RFD_CUDA(cudaStreamSynchronize(st));
+  return RFD_OK;
+}
+
+int32_t rfd_interval_class(int64_t n, const double* x, const double* a, const double* b,
+                           const double* A, double r2, int32_t dims, int32_t* cls) {
+  if (n < 0 || !x || !a || !b || !A || !cls || (dims != 2 && dims != 3))
+    return fail(RFD_ERR_ARG, "interval_class arguments");
+  for (int64_t e = 0; e < n; ++e) {
+    double di[3];
+    for (int k = 0; k < dims; ++k) di[k] = b[e * dims + k] - a[e * dims + k];
+    cls[e] = dims == 2 ? interval_class32<2>(x + e * dims, a + e * dims, di, A[e], r2)
+                       : interval_class32<3>(x + e * dims, a + e * dims, di, A[e], r2);
+  }
   return RFD_OK;
 }
 

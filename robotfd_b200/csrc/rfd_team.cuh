@@ -15,6 +15,7 @@
 #pragma once
 
 #include "rfd_device.cuh"
+#include "rfd_filter.h"
 
 namespace rfd {
 
@@ -28,7 +29,8 @@ struct TeamShared {
   int req_chunk[2];
   int cancel[2];
   int item_pair, item_strip, go, quit;
-  unsigned long long evaluated;
+  unsigned long long evaluated;    // cells the helpers computed
+  unsigned long long evaluated64;  // of those, cells with an interval computed in FP64
   int status;
   int pad;
 };
@@ -94,10 +96,11 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
   const int i = (s << 5) + lane;
   const bool rowv = i < R;
   const double r2 = st->r2;
+  const bool filt = KIND == K_DEC && st->filter;  // FP32 classification first (rfd_filter.h)
   RowData<KIND, D> row;
   if (rowv) row.load(pd, i);
   const long long t0 = clock64();
-  unsigned long long count = 0;
+  unsigned long long count = 0, count64 = 0;
   for (;;) {
     const int slot = seqH & 1;
     const long long tw0 = wa.prof ? clock64() : 0;
@@ -126,8 +129,26 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
       const bool ok = rowv && j >= 0 && j < C;
       if (KIND == K_DEC) {
         double rLB, rUB, tLB, tUB;
-        free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
-        free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+        // with the filter, an edge certainly empty or certainly whole takes the exact value
+        // the FP64 code would write; the others are computed in FP64
+        int cr = 0, ct = 0;
+        if (filt) {
+          cr = interval_class32<D>(row.b, col.qa, qd, col.A, r2);
+          ct = interval_class32<D>(col.qb, row.a, row.ab, row.A, r2);
+        }
+        if (cr == 0) {
+          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
+        } else {
+          rLB = cr == 1 ? -1.0 : 0.0;
+          rUB = cr == 1 ? -2.0 : 1.0;
+        }
+        if (ct == 0) {
+          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+        } else {
+          tLB = ct == 1 ? -1.0 : 0.0;
+          tUB = ct == 1 ? -2.0 : 1.0;
+        }
+        count64 += (ok && (cr == 0 || ct == 0)) ? 1 : 0;
         if (ok) {
           T0[(u << 5) + lane] = make_double2(rLB, rUB);
           T1[(u << 5) + lane] = make_double2(tLB, tUB);
@@ -157,8 +178,12 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     ++seqH;
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(kFull, count, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    count += __shfl_xor_sync(kFull, count, o);
+    count64 += __shfl_xor_sync(kFull, count64, o);
+  }
   if (lane == 0 && count) atomicAdd(&sh->evaluated, count);
+  if (lane == 0 && count64) atomicAdd(&sh->evaluated64, count64);
 }
 
 // ------------------------------------------------------------------ propagator (warp 0)
