@@ -13,6 +13,8 @@ free-space cells per decision.  Inputs are synthetic and seeded (the reference s
   plain : the plain method (bisection of [VE-FD, DFD], no bracket) on the same pair
   batch : the 4096-pair uneven batch (lognormal lengths, seed 2): learned and plain batched
           calls, and single-pair plain calls on a sample of it
+  mixed_precision : large 3D pairs with coordinates ~1e4, FP32 filter against FP64
+          (fraction of decision cells computed in FP64, error against the FP64 path)
   roofline : the dominant phase kernel against the measured FP64 FMA peak
   cpu_baseline : the CPU oracle (dense FP64 restatement, OpenMP) on a bounded sample,
                  extrapolated to the plain method's probes on the full pair
@@ -58,6 +60,8 @@ def parse():
     ap.add_argument("--points", type=int, default=200000,
                     help="points per curve of the long pair (smaller values: profiling cases)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4096-pair batch leg")
+    ap.add_argument("--mixed-pairs", type=int, default=2,
+                    help="pairs of the mixed-precision workload to solve (0: skip that leg)")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-method solves")
     ap.add_argument("--profile-batch", type=int, default=0, metavar="N",
                     help="profiling case: one batched call (one probe) on the first N pairs of "
@@ -229,6 +233,36 @@ def batch_leg(ctx, model, timed, sample=128):
                          "plain": max(r["probes"] for r in plain)},
         "max_rel_dev_learned_vs_plain": dev,
         "cells": sum(len(p) * len(q) for p, q in pairs),
+    }
+
+
+def mixed_leg(ctx, model, timed, npairs):
+    """The mixed-precision workload (config 4: large 3D spline pairs, coordinates ~1e4):
+    the first npairs pairs in one batched call with the bracket network, FP32 filter against
+    FP64 intervals."""
+    import robotfd_b200 as rfd
+    pairs = rfd.gen_config(4, npairs=npairs)
+    Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+    t64, r64 = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model), 1)
+    ctx.phase_times(enable=1)
+    t32, r32 = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
+                                                precision=rfd.RFD_PREC_FP32_FILTER), 1)
+    ph = ctx.phase_times(enable=0)
+    err = max(abs(a["distance"] - b["distance"]) / a["distance"] for a, b in zip(r64, r32))
+    ev = sum(r["cells_evaluated"] for r in r32)
+    return {
+        "workload": f"first {npairs} of 512 3D spline pairs (100k-400k points, waypoints "
+                    "U[-1e4,1e4]^3, seed 5), one batched call, bracket network",
+        "points": [[len(p), len(q)] for p, q in pairs],
+        "ms": {"fp64": sum(t64), "fp32_filter": sum(t32)},
+        "phase_ms_fp32_filter": {k: ph[k + "_ms"] for k in ("dfd", "vefd", "search")},
+        "probes": [r["probes"] for r in r32],
+        "decision_cells_evaluated": ev,
+        "decision_cells_fp64_fraction": sum(r["cells_fp64"] for r in r32) / max(ev, 1),
+        "max_rel_error_vs_fp64": err,
+        "decision_cells_per_s": {
+            "nominal": sum(r["cells_nominal"] for r in r32) / max(ph["search_ms"] * 1e-3, 1e-9),
+            "evaluated": ev / max(ph["search_ms"] * 1e-3, 1e-9)},
     }
 
 
@@ -414,6 +448,8 @@ def main():
     }
     if not args.no_batch:
         line["batch"] = batch_leg(ctx, model, timed)
+    if args.mixed_pairs > 0:
+        line["mixed_precision"] = mixed_leg(ctx, model, timed, args.mixed_pairs)
     if rank == 0:
         if world == 1:
             line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, pres["probes"])
