@@ -110,6 +110,22 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
 }
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
 
+// Boundary rows are filled with this pattern before every launch that hands rows between
+// strips (a NaN that no DP value takes: arithmetic makes canonical NaNs), so a consumer can
+// tell a value written in this launch from an old one without reading a flag first.
+constexpr unsigned long long kBndEmpty = ~0ull;
+
+// Relaxed (coherent, unordered) accesses of the handed-over rows.  No ordering with other
+// memory accesses is needed, so there is no compiler memory barrier.
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
+}
+
 // ------------------------------------------------------------------ cell arithmetic
 // Every operation is an explicit round-to-nearest intrinsic, so the result does not
 // depend on the compiler's contraction choices; the CPU oracle performs the same ops.

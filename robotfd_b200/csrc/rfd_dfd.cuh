@@ -42,7 +42,6 @@ struct DfdRing {
   static constexpr int cols = K <= 2 ? 128 : (K <= 4 ? 256 : 512);
   static_assert(cols >= 32 * K + 64, "ring too small");
 };
-constexpr unsigned long long kDfdEmpty = ~0ull;  // a NaN: "not yet written"
 
 template <bool B>
 struct BoolC {
@@ -51,18 +50,6 @@ struct BoolC {
 
 __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
 __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
-
-// Relaxed (coherent, unordered) accesses of the handed-over row.  No ordering with other
-// memory accesses is needed, so there is no compiler memory barrier: the shared-memory
-// reads of the steps stay free to be scheduled around the stores.
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
-  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v));
-}
 
 // Returns 0, or 1 on error / timeout (the error word is set).
 // SKEW: rows of a lane skewed by one column each (latency: independent cells per step), or
@@ -201,13 +188,13 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     // wait until every column of this chunk's input row has been written
     unsigned long long cur = nxt;
     for (int it = 0;; ++it) {
-      if (__all_sync(kFull, cur != kDfdEmpty)) break;
+      if (__all_sync(kFull, cur != kBndEmpty)) break;
       const int r = wt.check(it);
       if (r) {  // 1 cannot happen (the DFD has no dead strips); 2: error
         status = 1;
         break;
       }
-      if (cur == kDfdEmpty) cur = load_in(c);
+      if (cur == kBndEmpty) cur = load_in(c);
     }
     if (status) break;
     nxt = load_in(c + 1);  // in flight during this chunk

@@ -195,7 +195,23 @@ __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
     const long long n = (S - 1) * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
-      b[k] = make_ulonglong2(kDfdEmpty, kDfdEmpty);
+      b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
+  }
+}
+
+// Marks the boundary rows of the 32-row strips of every pair about to run `phase` as not
+// yet written (VE-FD and decision launches; see kBndEmpty).  Grid as dfd_fill_kernel.
+__global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int npairs, int phase) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int p = blockIdx.y; p < npairs; p += gridDim.y) {
+    if (st[p].phase != phase || !st[p].active) continue;
+    const PairDesc pd = pairs[p];
+    const long long S = (pd.n1 - 1 + 31) / 32;
+    if (S < 2) continue;
+    ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
+    const long long n = (S - 1) * pd.cstride / 2;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+      b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
   }
 }
 
@@ -570,7 +586,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0);
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * L.nlaunch);
-  const size_t prof_off = take(sizeof(unsigned long long) * 16);
+  const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
@@ -728,6 +744,13 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   wa.prof = ctx->prof ? (unsigned long long*)(dbase + prof_off) : nullptr;
   unsigned* counters = (unsigned*)(dbase + L.counters);
   int li = 0;
+  // boundary rows of the pairs about to run `ph` back to "not yet written" (team strips)
+  const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
+  const int fill_gx = std::max(1, 8 * ctx->num_sms / fill_gy);
+  auto fill = [&](int ph) {
+    bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dd, ds, (int)npairs, ph);
+    ++launches;
+  };
   if (mode != MODE_DECIDE) {
     wa.phase = PH_DFD;
     wa.ticket = counters + li++;
@@ -761,10 +784,12 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
       wa.phase = ph;
       wa.ticket = counters + li++;
-      if (ctx->solo)
+      if (ctx->solo) {
         wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
-      else
+      } else {
+        fill(ph);
         team_kernel<K_VEFD><<<ctx->team_grid[K_VEFD], kTeamThreads, team_smem_bytes<K_VEFD>(), st>>>(wa);
+      }
       RFD_CUDA(cudaGetLastError());
     }
     launches += 3;
@@ -790,10 +815,12 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   for (int k = 0; k < nprobe; ++k) {
     wa.phase = PH_SEARCH;
     wa.ticket = counters + li++;
-    if (ctx->solo)
+    if (ctx->solo) {
       wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
-    else
+    } else {
+      fill(PH_SEARCH);
       team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+    }
     RFD_CUDA(cudaGetLastError());
     ++launches;
   }
@@ -805,13 +832,32 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   RFD_CUDA(cudaStreamSynchronize(st));
   if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
   if (ctx->prof) {
-    unsigned long long pc[16];
-    RFD_CUDA(cudaMemcpy(pc, dbase + prof_off, sizeof(pc), cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> pc(kTraceBase + 3 * kTrace);
+    RFD_CUDA(cudaMemcpy(pc.data(), dbase + prof_off, sizeof(unsigned long long) * pc.size(),
+                        cudaMemcpyDeviceToHost));
     fprintf(stderr,
             "rfd prof (Mcycles): in_wait %.1f jump %.1f tile_wait %.1f steps %.1f strip_total %.1f |"
             " chunks %llu jumps %llu strips %llu | helpers: tile %.1f req_wait %.1f tiles %llu\n",
             pc[0] / 1e6, pc[1] / 1e6, pc[2] / 1e6, pc[3] / 1e6, pc[4] / 1e6, pc[5], pc[6], pc[7],
             pc[8] / 1e6, pc[9] / 1e6, pc[10]);
+    // strip chain of the first pair: handoff = first live input of strip s after the first
+    // live output of strip s-1; lag = first live output of strip s after its first live input
+    std::vector<double> hand, lag, adv;
+    const unsigned long long* tr = pc.data() + kTraceBase;
+    for (int s = 1; s < kTrace; ++s) {
+      const unsigned long long in = tr[3 * s + 1], out = tr[3 * s + 2], pout = tr[3 * (s - 1) + 2];
+      if (!in || !out || !pout) continue;
+      hand.push_back((double)in - (double)pout);
+      lag.push_back((double)out - (double)in);
+      adv.push_back((double)out - (double)pout);
+    }
+    auto med = [](std::vector<double> v) {
+      if (v.empty()) return 0.0;
+      std::sort(v.begin(), v.end());
+      return v[v.size() / 2];
+    };
+    fprintf(stderr, "rfd trace (ns, median over %zu strips): handoff %.0f  lag %.0f  advance %.0f\n",
+            hand.size(), med(hand), med(lag), med(adv));
   }
   if (ctx->timing) {
     float a = 0.f, b = 0.f, c = 0.f;
@@ -1312,6 +1358,8 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
       radius * radius);
   RFD_CUDA(cudaGetLastError());
   prep_kernel<<<1, 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH);
+  RFD_CUDA(cudaGetLastError());
+  bnd_fill_kernel<<<dim3(256, 1), 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH);
   RFD_CUDA(cudaGetLastError());
   WaveArgs wa;
   wa.pairs = ddesc;

@@ -188,6 +188,16 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
 
 // ------------------------------------------------------------------ propagator (warp 0)
 
+// RFD_PROF trace of the first kTrace strips of the first pair: wall-clock ns (globaltimer,
+// comparable across SMs) at strip start, first live input chunk, first live output flush.
+constexpr int kTrace = 512;
+constexpr int kTraceBase = 16;
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 template <int KIND, int D>
 __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState* st, const int s,
                                TeamShared* sh, const double2* tiles, unsigned& seqP,
@@ -214,6 +224,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   wt.start(wa, st, s);
   const long long t0 = clock64();
   if (wa.prof && lane == 0) atomicAdd(&wa.prof[7], 1ull);
+  unsigned long long* trace =
+      (wa.prof && st == wa.st && s < kTrace) ? wa.prof + kTraceBase + 3 * s : nullptr;
+  bool traced_in = false;
+  if (trace && lane == 0) trace[0] = global_ns();
 
   const int i = (s << 5) + lane;
   const bool rowv = i < R;
@@ -266,7 +280,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     const int col = (k << 5) + lane;
     double v = (k & 1) ? ob1 : ob0;
     const bool valid = col < C;
-    if (valid) __stcg(out_bnd + col, v);
+    if (valid) st_relaxed_f64(out_bnd + col, v);
     const unsigned live = __ballot_sync(kFull, valid && !is_dead<KIND>(v, U));
     if (k & 1) ob1 = dead_value<KIND>();
     else ob0 = dead_value<KIND>();
@@ -277,6 +291,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         if (first_live_out == kNone) {
           first_live_out = (unsigned)k;
           out_prog->first_live = (unsigned)k;
+          if (trace) trace[2] = global_ns();
         }
         out_prog->last_live = (unsigned)k;
       }
@@ -304,13 +319,33 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
   };
 
+  // The row above the strip for the next chunk is loaded during the current chunk's steps.
+  // The rows were filled with kBndEmpty before the launch and every word is written once, so
+  // a chunk whose 32 words are all written is final and is used at once, without the
+  // progress word or the tag; otherwise the flag protocol below decides.
+  unsigned long long pre = kBndEmpty;
+  int pre_c = -1;
+  auto prefetch = [&](int k) {
+    pre_c = -1;
+    if (!has_prod || (k << 5) >= C) return;
+    const int col = (k << 5) + lane;
+    pre = col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dead_value<KIND>());
+    pre_c = k;
+  };
+
   int c = 0;
   while (!dead_tail && (c << 5) < nsteps) {
     if (has_cons)
       while (next_flush <= c - 2) flush(next_flush++);
     double inreg = dead_value<KIND>();
     bool in_live = false;
-    if ((c << 5) < C) {
+    bool fast = false;
+    if (has_prod && pre_c == c && __all_sync(kFull, pre != kBndEmpty)) {
+      inreg = __longlong_as_double(pre);
+      in_live = __any_sync(kFull, ((c << 5) + lane) < C && !is_dead<KIND>(inreg, U));
+      fast = true;
+    }
+    if (!fast && (c << 5) < C) {
       if (has_prod) {
         unsigned long long w;
         const int r = wait_cols((unsigned)min((c + 1) << 5, C), w);
@@ -325,6 +360,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       } else {
         in_live = !is_dead<KIND>(inreg, U);
       }
+    }
+    if (trace && in_live && !traced_in) {
+      traced_in = true;
+      if (lane == 0) trace[1] = global_ns();
     }
     if (!dense && !in_live) {
       const bool ldead = (!rowv || is_dead<KIND>(bot, U) || ((c << 5) - lane >= C)) &&
@@ -397,6 +436,11 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         }
         if (has_cons) {
           next_flush = nc - 1;
+          // Liveness enters a strip only through its input row, so no output chunk before
+          // nc can be live: publish nc as a lower bound of the first live output chunk
+          // (the flush of the actual one overwrites it).  The next strip then starts its
+          // cold-start tile now instead of when that chunk is flushed.
+          if (lane == 0 && first_live_out == kNone) out_prog->first_live = (unsigned)nc;
           publish_cols(min((nc - 1) << 5, C));
         }
         carry = dead_value<KIND>();
@@ -424,6 +468,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
     const double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
     const double2* T1 = T0 + 1024;
+    prefetch(c + 1);
     const long long ts0 = wa.prof ? clock64() : 0;
 #pragma unroll
     for (int u = 0; u < 32; ++u) {
