@@ -340,10 +340,31 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     double inreg = dead_value<KIND>();
     bool in_live = false;
     bool fast = false;
-    if (has_prod && pre_c == c && __all_sync(kFull, pre != kBndEmpty)) {
-      inreg = __longlong_as_double(pre);
-      in_live = __any_sync(kFull, ((c << 5) + lane) < C && !is_dead<KIND>(inreg, U));
-      fast = true;
+    if (has_prod && (c << 5) < C) {
+      // Poll the chunk's words themselves (and, alongside, the progress word): a complete
+      // chunk is used as soon as it lands.  A chunk the progress word calls final while
+      // words are still missing was skipped (dead) or read early: the flag protocol below
+      // settles it, as it does a dead strip or an expired wait.
+      const int col = (c << 5) + lane;
+      const unsigned need = (unsigned)min((c + 1) << 5, C);
+      auto load = [&]() {
+        return col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dead_value<KIND>());
+      };
+      unsigned long long v = pre_c == c ? pre : load();
+      unsigned long long w = 0ull;
+      for (int it = 0;; ++it) {
+        if (__all_sync(kFull, v != kBndEmpty)) {
+          inreg = __longlong_as_double(v);
+          in_live = __any_sync(kFull, col < C && !is_dead<KIND>(inreg, U));
+          fast = true;
+          break;
+        }
+        if (it > 0 && (unsigned)(w >> 32) == E && (unsigned)(w & 0xffffffffu) >= need) break;
+        if (wt.check(it)) break;
+        if (lane == 0) w = ld_relaxed_u64(&in_prog->word);  // both loads in flight together
+        if (v == kBndEmpty) v = load();
+        w = bcast(w);
+      }
     }
     if (!fast && (c << 5) < C) {
       if (has_prod) {
@@ -401,6 +422,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
                 if (b) nc = pos + __ffs(b) - 1;
                 else pos = min(pos + 32, end);
               }
+              // No chunk before the producer's first live chunk is live, and the producer
+              // writes every chunk from there on: go to it now and wait for its words in
+              // the input path (a chunk that turns out dead just jumps again).
+              if (nc < 0 && !done && pos < nout) nc = pos;
               // The producer's first live chunk at or after pos is where this strip will
               // most likely resume: start its tile now so it is ready at the jump.
               if (nc < 0 && pos < nout && pending != pos) {
