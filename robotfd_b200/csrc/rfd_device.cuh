@@ -192,6 +192,16 @@ __device__ __forceinline__ void free_interval(const double* x, const double* a, 
   }
 }
 
+// Compare-and-select minimum / maximum, on the dependency chain of the sweeps in place of
+// fmin / fmax (whose NaN handling costs several instructions of latency).  They agree with
+// fmin / fmax whenever neither operand is NaN, which holds for every value the sweeps
+// propagate from finite coordinates: DFD and VE-FD values are squared distances (a
+// degenerate segment clamps its parameter with fmax / fmin, which drop the NaN), and free
+// intervals are finished by fmax / fmin in free_interval.  Signs of zero may differ only
+// in interval lower bounds, which enter comparisons alone (-0 == +0).
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+
 // ------------------------------------------------------------------ per-kind policy
 
 template <int KIND>

@@ -48,8 +48,6 @@ struct BoolC {
   static constexpr bool value = B;
 };
 
-__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
-__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
 
 // Returns 0, or 1 on error / timeout (the error word is set).
 // SKEW: rows of a lane skewed by one column each (latency: independent cells per step), or

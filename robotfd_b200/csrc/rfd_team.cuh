@@ -325,6 +325,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // progress word or the tag; otherwise the flag protocol below decides.
   unsigned long long pre = kBndEmpty;
   int pre_c = -1;
+  bool seen_live = false;  // has a live input chunk reached this strip yet
   auto prefetch = [&](int k) {
     pre_c = -1;
     if (!has_prod || (k << 5) >= C) return;
@@ -382,6 +383,18 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         in_live = !is_dead<KIND>(inreg, U);
       }
     }
+    if (in_live && !seen_live) {
+      seen_live = true;
+      // Liveness enters a strip only through its input row, so no output chunk before c can
+      // be live: publish c as a lower bound of the first live output chunk (the flush of the
+      // actual one overwrites it), so the next strip moves to this strip's band and starts
+      // its tile about two chunks before that flush.  Any value the consumer reads is a valid
+      // lower bound, so no release is needed.
+      if (has_cons && lane == 0 && first_live_out == kNone) {
+        out_prog->first_live = (unsigned)c;
+        __threadfence();
+      }
+    }
     if (trace && in_live && !traced_in) {
       traced_in = true;
       if (lane == 0) trace[1] = global_ns();
@@ -423,9 +436,11 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
                 else pos = min(pos + 32, end);
               }
               // No chunk before the producer's first live chunk is live, and the producer
-              // writes every chunk from there on: go to it now and wait for its words in
-              // the input path (a chunk that turns out dead just jumps again).
-              if (nc < 0 && !done && pos < nout) nc = pos;
+              // writes every chunk from there on: until this strip has seen live input, go
+              // to the next candidate chunk now and wait for its words in the input path (a
+              // chunk that turns out dead moves on by one).  After the band has passed, the
+              // tag scan finds the next live chunk, 32 at a time.
+              if (nc < 0 && !done && pos < nout && !seen_live) nc = pos;
               // The producer's first live chunk at or after pos is where this strip will
               // most likely resume: start its tile now so it is ready at the jump.
               if (nc < 0 && pos < nout && pending != pos) {
@@ -461,11 +476,6 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         }
         if (has_cons) {
           next_flush = nc - 1;
-          // Liveness enters a strip only through its input row, so no output chunk before
-          // nc can be live: publish nc as a lower bound of the first live output chunk
-          // (the flush of the actual one overwrites it).  The next strip then starts its
-          // cold-start tile now instead of when that chunk is flushed.
-          if (lane == 0 && first_live_out == kNone) out_prog->first_live = (unsigned)nc;
           publish_cols(min((nc - 1) << 5, C));
         }
         carry = dead_value<KIND>();
@@ -512,18 +522,18 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         const bool bdead = bot < 0.0, ldead = left < 0.0;
         const bool rinv = (left > rUB) || ldead;
         const bool tinv = (bot > tUB) || bdead;
-        const double rm = fmax(rLB, left);
-        const double tm = fmax(tLB, bot);
+        const double rm = dmax(rLB, left);
+        const double tm = dmax(tLB, bot);
         ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
         nres = bdead ? (rinv ? -2.0 : rUB) : rUB;
         nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
       } else {
-        const double in = fmin(left, bot);
-        const double top = fmax(ta.x, in);
-        const double right = fmax(ta.y, in);
+        const double in = dmin(left, bot);
+        const double top = dmax(ta.x, in);
+        const double right = dmax(ta.y, in);
         ncarry = right;
         nbot = top;
-        nres = fmin(top, right);
+        nres = dmin(top, right);
       }
       carry = act ? ncarry : carry;
       bot = act ? nbot : bot;
