@@ -745,8 +745,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   unsigned* counters = (unsigned*)(dbase + L.counters);
   int li = 0;
   // boundary rows of the pairs about to run `ph` back to "not yet written" (team strips)
+  // (at least 32 blocks per pair: late probe rounds leave a few large pairs active)
   const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
-  const int fill_gx = std::max(1, 8 * ctx->num_sms / fill_gy);
+  const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
   auto fill = [&](int ph) {
     bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dd, ds, (int)npairs, ph);
     ++launches;
