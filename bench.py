@@ -42,6 +42,7 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
 DEC_DRAM_BYTES_20K = 2.408192e6
+COARSE_UB = 4  # the learned form's upper bound: inflated DFD of every 4th point (rfd.h coarse_ub)
 DFD_DRAM_BYTES_200K = 1.10e9 + 1.20e9
 KERNEL_OF_PHASE = {"dfd": "dfd_kernel<8>", "vefd": "team_kernel<K_VEFD>",
                    "search": "team_kernel<K_DEC>"}
@@ -210,6 +211,8 @@ def batch_leg(ctx, model, timed, sample=128):
     n = len(Ps)
     ctx.distance_batch(Ps[:64], Qs[:64], precise=True, model=model)  # warm
     t_l, learned = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model), 2)
+    t_c, _ = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
+                                              coarse_ub=COARSE_UB), 1)
     t_p, plain = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True), 1)
     idx = list(range(0, n, max(1, n // sample)))[:sample]
     t_s, single = timed(lambda: [ctx.distance(Ps[k], Qs[k], precise=True) for k in idx], 1)
@@ -219,6 +222,7 @@ def batch_leg(ctx, model, timed, sample=128):
     for k, r in zip(idx, single):
         assert r["distance"] == plain[k]["distance"], "single and batched plain results differ"
     sps = {"learned_batched": n / (statistics.median(t_l) * 1e-3),
+           "learned_batched_coarse_ub": n / (t_c[0] * 1e-3),
            "plain_batched": n / (statistics.median(t_p) * 1e-3),
            "plain_single_calls": len(idx) / (sum(t_s) * 1e-3)}
     return {
@@ -299,10 +303,10 @@ def main():
 
     def step_dev():
         return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True,
-                                   model=model)
+                                   model=model, coarse_ub=COARSE_UB)
 
     def step_host():
-        return ctx.distance(P, Q, precise=True, model=model)
+        return ctx.distance(P, Q, precise=True, model=model, coarse_ub=COARSE_UB)
 
     def step_plain():
         return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True)
@@ -404,7 +408,8 @@ def main():
         "data": "synthetic",
         "config": {"workload": WORKLOAD if args.points == 200000 else
                    f"long-pair generator at {args.points} points per curve", "n1": n1, "n2": n2,
-                   "dims": d, "stop": "ub-lb <= 2^-33 ub", "form": "learned bracket (shipped network)",
+                   "dims": d, "stop": "ub-lb <= 2^-33 ub",
+                   "form": f"learned bracket (shipped network), coarse upper bound k={COARSE_UB}",
                    "parallelism": f"replicas x{world}",
                    "l2": "flushed before every step (256 MiB write outside the timed events)"},
         "fd": res["distance"],

@@ -56,7 +56,8 @@ enum rfd_flag {
   RFD_FLAG_VEFD_DENSE = 16,    /* VE-FD pruning bound was too tight, recomputed without pruning */
   RFD_FLAG_BRACKET_USED = 32,  /* a proposed bracket was verified and used */
   RFD_FLAG_BRACKET_WIDENED = 64, /* a proposed bracket failed verification and was widened */
-  RFD_FLAG_DEGENERATE = 128    /* a curve of one point: closed form used */
+  RFD_FLAG_DEGENERATE = 128,   /* a curve of one point: closed form used */
+  RFD_FLAG_DFD_COARSE = 256    /* dfd holds the coarse upper bound (rfd_options.coarse_ub) */
 };
 
 typedef struct rfd_model rfd_model;
@@ -74,6 +75,14 @@ typedef struct rfd_options {
                                distance; verified by two decisions, widened on failure */
   const rfd_model* model;   /* optional learned bracket: proposes [lo, hi] per pair from the
                                curves and the VE-FD bound (ignored when bracket is set) */
+  int32_t coarse_ub;        /* 0: the DFD is the upper bound (the reference's method).  k in
+                               [2, 4096] (needs reference_quirks = 0): the upper bound is the DFD of
+                               every k-th point and the last, each cell weighted by the distance
+                               plus both points' inflations (the largest distance of a point of an
+                               adjacent block to its block's end points): a certified bound on
+                               the DFD from k*k times fewer cells.  result.dfd then holds that
+                               bound (RFD_FLAG_DFD_COARSE).  The FD, within the stop rule, does
+                               not depend on it. */
 } rfd_options;
 
 typedef struct rfd_result {

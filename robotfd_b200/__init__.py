@@ -41,6 +41,7 @@ FLAG_VEFD_DENSE = 16
 FLAG_BRACKET_USED = 32
 FLAG_BRACKET_WIDENED = 64
 FLAG_DEGENERATE = 128
+FLAG_DFD_COARSE = 256
 
 FLT_EPSILON = float(np.finfo(np.float32).eps)
 REL_TOL = 2.0 ** -33
@@ -75,6 +76,7 @@ class Options(ctypes.Structure):
         ("memory", ctypes.c_int32),
         ("bracket", ctypes.POINTER(ctypes.c_double)),
         ("model", ctypes.c_void_p),
+        ("coarse_ub", ctypes.c_int32),
     ]
 
 
@@ -204,7 +206,7 @@ def _curve(c):
 
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
-            precision=RFD_PREC_FP64, model=None):
+            precision=RFD_PREC_FP64, model=None, coarse_ub=0):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -217,6 +219,7 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
         o.reference_quirks = int(bool(quirks))
     if model is not None:
         o.model = model._h.value
+    o.coarse_ub = int(coarse_ub)
     return o
 
 

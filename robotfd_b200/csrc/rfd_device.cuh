@@ -77,7 +77,7 @@ struct PairState {
   int dead_from, done_count;
   int use_model;
   int filter;  // 1: decision intervals through the FP32 filter (RFD_PREC_FP32_FILTER)
-  int pad;
+  int coarse;  // 1: the DFD phase computes the coarse upper bound (rfd_options.coarse_ub)
 };
 
 template <int D>

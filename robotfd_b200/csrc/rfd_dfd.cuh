@@ -49,12 +49,27 @@ struct BoolC {
 };
 
 
+// Cell weight: the squared point distance, or with INFL (the coarse upper bound,
+// rfd_options.coarse_ub) the squared sum of the point distance and the two points' inflations
+// (stored as coordinate D), each operation rounded to nearest; the bound built from it is
+// widened by a relative margin that covers these roundings.
+template <int D, bool INFL>
+__device__ __forceinline__ double cell_weight(const double* p, const double* q) {
+  const double s = dist_sq<D>(p, q);
+  if (!INFL) return s;
+  const double e = __dadd_rn(__dadd_rn(__dsqrt_rn(s), p[D]), q[D]);
+  return __dmul_rn(e, e);
+}
+
 // Returns 0, or 1 on error / timeout (the error word is set).
 // SKEW: rows of a lane skewed by one column each (latency: independent cells per step), or
 // all at the lane's column (throughput: fewer instructions per cell, no point passing).
-template <int D, int K, bool SKEW>
+// INFL: points carry an inflation as coordinate D (stride D + 1) and the weight of a cell is
+// cell_weight<D, true>.
+template <int D, int K, bool SKEW, bool INFL = false>
 __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, const int s,
-                         double* ring /* [3][DfdRing<K>::cols] per warp */) {
+                         double* ring /* [D + INFL][DfdRing<K>::cols] per warp */) {
+  constexpr int DS = D + (INFL ? 1 : 0);  // stride of a point
   constexpr int H = 32 * K;
   constexpr int RC = DfdRing<K>::cols;
   const int lane = threadIdx.x & 31;
@@ -71,12 +86,12 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   // rows of this lane (clamped loads beyond the last row: their values are never used)
   const int base = SKEW ? lane * K : lane;  // row k of this lane is at column t - base - k*SKEW
   const int i0 = s * H + lane * K;
-  double p[K][D];
+  double p[K][DS];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int row = min(i0 + k, R - 1);
 #pragma unroll
-    for (int e = 0; e < D; ++e) p[k][e] = __ldg(pd.P + (size_t)row * D + e);
+    for (int e = 0; e < DS; ++e) p[k][e] = __ldg(pd.P + (size_t)row * DS + e);
   }
   const int rlast = R - 1 - i0;  // index k of the pair's last row when this lane holds it
   const bool holds_last = s == S - 1 && rlast >= 0 && rlast < K;
@@ -84,27 +99,27 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   const int tres = C - 1 + base + (SKEW ? rlast : 0);
   constexpr int kOutLag = SKEW ? H - 1 : 31;  // column of the last row = t - kOutLag
 
-  double bot[K], carry[K], qp[K][D];
+  double bot[K], carry[K], qp[K][DS];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     bot[k] = kFltMax;
     carry[k] = kFltMax;
 #pragma unroll
-    for (int e = 0; e < D; ++e) qp[k][e] = 0.0;
+    for (int e = 0; e < DS; ++e) qp[k][e] = 0.0;
   }
   double res = kFltMax;
   const int nsteps = C + kOutLag;
   int status = 0;
 
-  auto stage = [&](int c, const double (&q)[D]) {
+  auto stage = [&](int c, const double (&q)[DS]) {
     const int slot = ((c << 5) + lane) & (RC - 1);
 #pragma unroll
-    for (int e = 0; e < D; ++e) ring[e * RC + slot] = q[e];
+    for (int e = 0; e < DS; ++e) ring[e * RC + slot] = q[e];
   };
-  auto fetch = [&](int c, double (&q)[D]) {
+  auto fetch = [&](int c, double (&q)[DS]) {
     const int j = min((c << 5) + lane, C - 1);
 #pragma unroll
-    for (int e = 0; e < D; ++e) q[e] = __ldg(pd.Q + (size_t)j * D + e);
+    for (int e = 0; e < DS; ++e) q[e] = __ldg(pd.Q + (size_t)j * DS + e);
   };
   // the row above the strip at column 32c + lane (empty pattern while not yet written)
   auto load_in = [&](int c) -> unsigned long long {
@@ -129,26 +144,26 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
       const double lin = __shfl_sync(kFull, inreg, u);
       const double lup = __shfl_up_sync(kFull, carry[K - 1], 1);
       const double left0 = lane == 0 ? lin : lup;
-      double q0[D];
+      double q0[DS];
       const int slot = (t - base) & (RC - 1);
 #pragma unroll
-      for (int e = 0; e < D; ++e) q0[e] = ring[e * RC + slot];
+      for (int e = 0; e < DS; ++e) q0[e] = ring[e * RC + slot];
       if (SKEW) {
         // rows in descending order: row k reads row k-1's values of the previous step
 #pragma unroll
         for (int k = K - 1; k >= 0; --k) {
-          double q[D];
+          double q[DS];
 #pragma unroll
-          for (int e = 0; e < D; ++e) q[e] = k == 0 ? q0[e] : qp[k - 1][e];
+          for (int e = 0; e < DS; ++e) q[e] = k == 0 ? q0[e] : qp[k - 1][e];
           const double left = k == 0 ? left0 : carry[k - 1];
-          const double dist = dist_sq<D>(p[k], q);
+          const double dist = cell_weight<D, INFL>(p[k], q);
           const double b = (FIRST && t - base - k == 0) ? kFltMax : bot[k];
           const double in = dmin(left, b);
           const double top = dmax(dist, in);
           carry[k] = dmin(top, b);
           bot[k] = top;
 #pragma unroll
-          for (int e = 0; e < D; ++e) qp[k][e] = q[e];
+          for (int e = 0; e < DS; ++e) qp[k][e] = q[e];
         }
       } else {
         // rows in ascending order at one column: each takes the row below's carry
@@ -156,7 +171,7 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
         const bool j0 = FIRST && t - base == 0;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const double dist = dist_sq<D>(p[k], q0);
+          const double dist = cell_weight<D, INFL>(p[k], q0);
           const double b = j0 ? kFltMax : bot[k];
           const double in = dmin(left, b);
           const double top = dmax(dist, in);
@@ -175,7 +190,7 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     }
   };
 
-  double qn[D];
+  double qn[DS];
   fetch(0, qn);
   stage(0, qn);
   __syncwarp();

@@ -93,8 +93,15 @@ __device__ __forceinline__ void begin_search(PairState* st, int* active_pairs,
 
 template <int KIND>
 __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
-  const double r = *(volatile double*)&st->result;
+  double r = *(volatile double*)&st->result;
   if (KIND == K_DFD) {
+    if (st->coarse) {
+      // coarse upper bound: the inflated DFD of the anchors, widened by a margin that covers
+      // the roundings of its weights
+      const double ub = __dmul_rn(__dsqrt_rn(r), 1.0 + 0x1p-40);
+      r = __dmul_rn(ub, ub);
+      st->flags |= RFD_FLAG_DFD_COARSE;
+    }
     st->dfd = __dsqrt_rn(r);  // reference .cu:633
     if (pd.n1 < 2 || pd.n2 < 2) {
       // one-point curve: every coupling maps the other curve onto that point
@@ -182,6 +189,56 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
   }
 }
 
+// Coarse upper bound (rfd_options.coarse_ub = k), step 1: the anchors (every k-th point
+// and the last) of both curves into the coarse pair's arrays, with an inflation as extra
+// coordinate: the largest distance from a point of either block next to the anchor to the
+// end points of its block.  A monotone coupling of the anchors extends, block by block, to
+// the full point sequences, each full pair lying within the inflations of a coupled anchor
+// pair; so the DFD of the anchors with cell weights (|a - b| + inflation(a) + inflation(b))^2
+// is at least the DFD of the curves.  One block per pair (grid-stride); pairs with
+// coarse = 0 keep the DFD.
+__global__ void coarse_prep_kernel(const PairDesc* pairs, const PairDesc* coarse, PairState* st,
+                                   int npairs, int k) {
+  for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
+    // a pair with a one-point curve (coarse = 0): every point, inflation 0, so the inflated
+    // sweep computes its exact DFD
+    const bool exact = !st[p].coarse;
+    const PairDesc pd = pairs[p], cd = coarse[p];
+    const int d = pd.d, ds = d + 1;
+    for (int side = 0; side < 2; ++side) {
+      const double* X = side ? pd.Q : pd.P;
+      double* Y = const_cast<double*>(side ? cd.Q : cd.P);
+      const long long n = side ? pd.n2 : pd.n1, cn = side ? cd.n2 : cd.n1;
+      auto anchor = [&](long long a) { return exact ? a : (a == cn - 1 ? n - 1 : a * k); };
+      // largest distance from a point of block b (anchors b, b+1) to the block's end points
+      auto block_span = [&](long long b) {
+        const long long lo = anchor(b), hi = anchor(b + 1);
+        double m = 0.0;
+        for (long long i = lo; i <= hi; ++i) {
+          double d1 = 0.0, d2 = 0.0;
+          for (int e = 0; e < d; ++e) {
+            const double t1 = __dsub_rn(X[i * d + e], X[lo * d + e]);
+            const double t2 = __dsub_rn(X[i * d + e], X[hi * d + e]);
+            d1 = __fma_rn(t1, t1, d1);
+            d2 = __fma_rn(t2, t2, d2);
+          }
+          m = fmax(m, fmax(d1, d2));
+        }
+        return __dsqrt_rn(m);
+      };
+      // each anchor: its coordinates and the larger span of its two blocks (each block's span
+      // is computed by both of its anchors: no thread reads another's result)
+      for (long long a = threadIdx.x; a < cn; a += blockDim.x) {
+        const long long at = anchor(a);
+        for (int e = 0; e < d; ++e) Y[a * ds + e] = X[at * d + e];
+        const double left = !exact && a > 0 ? block_span(a - 1) : 0.0;
+        const double right = !exact && a + 1 < cn ? block_span(a) : 0.0;
+        Y[a * ds + d] = fmax(left, right);
+      }
+    }
+  }
+}
+
 // Marks the rows the DFD strips of 32*K rows hand to each other as not yet written (the
 // all-ones pattern, a NaN no DFD value takes).  Pairs are spread over grid rows (y) and
 // each pair's rows over grid columns (x), so one large pair uses every SM.
@@ -218,9 +275,9 @@ __global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int 
 // Dense DFD strips of 32*K rows (rfd_dfd.cuh), same in-order ticket scheme as wave_kernel
 // over the (pair, 32-row strip) item list: item (p, s) is strip s of 32*K rows, items past
 // the pair's last tall strip are skipped.
-template <int K, bool SKEW>
+template <int K, bool SKEW, bool INFL = false>
 __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
-  __shared__ double ring[kBlock / 32][3 * DfdRing<K>::cols];
+  __shared__ double ring[kBlock / 32][(INFL ? 4 : 3) * DfdRing<K>::cols];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (bcast(lane == 0 ? ld_volatile(wa.active_pairs) : 0) == 0) return;
   for (;;) {
@@ -239,8 +296,8 @@ __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
     const PairDesc pd = wa.pairs[it.x];
     const int S = (pd.n1 + 32 * K - 1) / (32 * K);
     if (it.y >= S) continue;
-    const int status = pd.d == 2 ? dfd_strip<2, K, SKEW>(wa, pd, st, it.y, ring[warp])
-                                 : dfd_strip<3, K, SKEW>(wa, pd, st, it.y, ring[warp]);
+    const int status = pd.d == 2 ? dfd_strip<2, K, SKEW, INFL>(wa, pd, st, it.y, ring[warp])
+                                 : dfd_strip<3, K, SKEW, INFL>(wa, pd, st, it.y, ring[warp]);
     if (status) return;
     __syncwarp();
     if (lane == 0) {
@@ -465,6 +522,7 @@ struct rfd_context {
   int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
   int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
   int dfd_grid[2] = {0, 0};  // [stacked, skewed]
+  int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 4 rows per lane
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
   size_t dws_size = 0;
@@ -550,6 +608,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (!(o.tol >= 0.0)) return fail(RFD_ERR_ARG, "tol");
   if (o.precision != RFD_PREC_FP64 && o.precision != RFD_PREC_FP32_FILTER)
     return fail(RFD_ERR_ARG, "precision");
+  if (o.coarse_ub < 0 || o.coarse_ub == 1 || o.coarse_ub > 4096)
+    return fail(RFD_ERR_ARG, "coarse_ub must be 0 or in [2, 4096]");
+  if (o.coarse_ub && o.reference_quirks)
+    return fail(RFD_ERR_ARG, "coarse_ub needs reference_quirks = 0 (the quirk reads the DFD sizes)");
   for (int64_t p = 0; p < npairs; ++p) {
     int rc = check_pair(c1s[p], n1s[p], c2s[p], n2s[p], dims[p]);
     if (rc) return rc;
@@ -564,9 +626,13 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.P.resize(npairs); L.Q.resize(npairs); L.rowc.resize(npairs); L.colrec.resize(npairs);
   L.bnd.resize(npairs); L.tags.resize(npairs); L.prog.resize(npairs);
   L.hP.resize(npairs); L.hQ.resize(npairs);
+  const int ck = mode == MODE_DISTANCE ? o.coarse_ub : 0;  // coarse upper bound, every ck-th point
+  auto coarse_n = [&](int64_t n) { return n < 2 ? n : (n - 2) / ck + 2; };  // anchors 0, ck, ..., n-1
+  std::vector<size_t> cP(ck ? npairs : 0), cQ(ck ? npairs : 0);
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t r = off; off = align_up(off + bytes, 256); return r; };
   L.descs = take(sizeof(PairDesc) * npairs);
+  const size_t cdescs = ck ? take(sizeof(PairDesc) * npairs) : 0;
   L.states = take(sizeof(PairState) * npairs);
   // items: interleave pairs by strip index so early strips of every pair go first
   std::vector<int> order(npairs);
@@ -613,12 +679,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(n1 - 1, 1));
     L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(n2 - 1, 1));
     L.bnd[p] = take(sizeof(double) * (S > 1 ? S - 1 : 0) * cstride);
+    if (ck) {
+      // anchors and their inflations; a pair with a one-point curve keeps every point, with
+      // inflation 0 (its DFD is its exact, closed-form answer)
+      const bool full = n1 < 2 || n2 < 2;
+      cP[p] = take(sizeof(double) * (full ? n1 : coarse_n(n1)) * (d + 1));
+      cQ[p] = take(sizeof(double) * (full ? n2 : coarse_n(n2)) * (d + 1));
+    }
   }
   L.total = off;
 
   size_t hoff = 0;
   auto htake = [&](size_t bytes) { size_t r = hoff; hoff = align_up(hoff + bytes, 256); return r; };
   L.h_descs = htake(sizeof(PairDesc) * npairs);
+  const size_t h_cdescs = ck ? htake(sizeof(PairDesc) * npairs) : 0;
   L.h_states = htake(sizeof(PairState) * npairs);
   L.h_items = htake(sizeof(int2) * nitems);
   L.h_misc = htake(4 * sizeof(int));
@@ -668,6 +742,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     D.cstride = (long long)align_up((size_t)n2, 32);
     D.tstride = (long long)align_up((size_t)((n2 + 31) / 32), 32);
     (void)S;
+    if (ck) {
+      // the coarse pair: anchors of both curves, handing rows over through the pair's own
+      // boundary rows (fewer rows of fewer columns).  A one-point curve keeps the exact DFD,
+      // which is its closed-form answer.
+      PairDesc& Dc = ((PairDesc*)(hbase + h_cdescs))[p];
+      Dc = D;
+      Dc.P = (const double*)(dbase + cP[p]);
+      Dc.Q = (const double*)(dbase + cQ[p]);
+      if (n1 >= 2 && n2 >= 2) {
+        Dc.n1 = (int)coarse_n(n1);
+        Dc.n2 = (int)coarse_n(n2);
+        Dc.cstride = (long long)align_up((size_t)Dc.n2, 32);
+      }
+    }
     PairState& s = hs[p];
     memset(&s, 0, sizeof(s));
     s.srch.tol = o.tol;
@@ -678,6 +766,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     s.use_model = use_model ? 1 : 0;
     s.filter = o.precision == RFD_PREC_FP32_FILTER ? 1 : 0;
     s.blo = s.bhi = NAN;
+    s.coarse = (ck && n1 >= 2 && n2 >= 2) ? 1 : 0;
     if (o.bracket && mode == MODE_DISTANCE) {
       s.blo = o.bracket[2 * p];
       s.bhi = o.bracket[2 * p + 1];
@@ -705,6 +794,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     for (int64_t p = 0; p < npairs; ++p) h2d_bytes += sizeof(double) * (n1s[p] + n2s[p]) * dims[p];
   RFD_CUDA(cudaMemcpyAsync(dbase + L.descs, hbase + L.h_descs, sizeof(PairDesc) * npairs,
                            cudaMemcpyHostToDevice, st));
+  if (ck) {
+    RFD_CUDA(cudaMemcpyAsync(dbase + cdescs, hbase + h_cdescs, sizeof(PairDesc) * npairs,
+                             cudaMemcpyHostToDevice, st));
+    h2d_bytes += sizeof(PairDesc) * npairs;
+  }
   RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * npairs,
                            cudaMemcpyHostToDevice, st));
   RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
@@ -755,21 +849,37 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (mode != MODE_DECIDE) {
     wa.phase = PH_DFD;
     wa.ticket = counters + li++;
+    // the DFD sweep runs on the coarse pairs when the coarse upper bound is asked for
+    const PairDesc* ddfd = ck ? (const PairDesc*)(dbase + cdescs) : dd;
+    if (ck) {
+      coarse_prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(
+          dd, ddfd, ds, (int)npairs, ck);
+      ++launches;
+    }
+    // the inflated (coarse) sweep always runs 4 rows per lane (its point records are wider)
+    const int rows = ck ? 4 : ctx->dfd_rows;
     {
       const int gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
-      const int gx = std::max(1, 8 * ctx->num_sms / gy);
-      dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(dd, (int)npairs, 32 * ctx->dfd_rows);
+      const int gx = std::max(32, 8 * ctx->num_sms / gy);
+      dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(ddfd, (int)npairs, 32 * rows);
     }
     ++launches;
+    wa.pairs = ddfd;
     {
       // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
       // latency decides), stacked rows otherwise (instruction throughput decides)
       int64_t strips = 0;
-      for (int64_t p = 0; p < npairs; ++p) strips += (n1s[p] + 32 * ctx->dfd_rows - 1) / (32 * ctx->dfd_rows);
+      for (int64_t p = 0; p < npairs; ++p) {
+        const int64_t n1 = ck && n1s[p] >= 2 && n2s[p] >= 2 ? coarse_n(n1s[p]) : n1s[p];
+        strips += (n1 + 32 * rows - 1) / (32 * rows);
+      }
+      const int* grid = ck ? ctx->dfd_grid_infl : ctx->dfd_grid;
       const int sk = ctx->dfd_skew >= 0 ? ctx->dfd_skew
-                                         : (strips < 2 * (int64_t)ctx->dfd_grid[1] * (kBlock / 32) ? 1 : 0);
-      const int g = ctx->dfd_grid[sk];
-      switch (ctx->dfd_rows * 2 + sk) {
+                                         : (strips < 2 * (int64_t)grid[1] * (kBlock / 32) ? 1 : 0);
+      const int g = grid[sk];
+      switch (ck ? 100 + sk : ctx->dfd_rows * 2 + sk) {
+        case 100: dfd_kernel<4, false, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 101: dfd_kernel<4, true, true><<<g, kBlock, 0, st>>>(wa); break;
         case 2: dfd_kernel<1, false><<<g, kBlock, 0, st>>>(wa); break;
         case 3: dfd_kernel<1, true><<<g, kBlock, 0, st>>>(wa); break;
         case 4: dfd_kernel<2, false><<<g, kBlock, 0, st>>>(wa); break;
@@ -780,6 +890,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         default: dfd_kernel<8, true><<<g, kBlock, 0, st>>>(wa); break;
       }
     }
+    wa.pairs = dd;
     RFD_CUDA(cudaGetLastError());
     if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
     for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
@@ -999,6 +1110,10 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
         default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, true>, kBlock, 0); break;
       }
       c->dfd_grid[sk] = std::max(1, od) * c->num_sms;
+      od = 0;
+      if (sk) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, true, true>, kBlock, 0);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, false, true>, kBlock, 0);
+      c->dfd_grid_infl[sk] = std::max(1, od) * c->num_sms;
     }
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';

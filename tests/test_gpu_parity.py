@@ -204,3 +204,35 @@ def test_dfd_rows_per_lane_bitexact(built, rows, skew):
                 assert dfd == np.sqrt(oracle.dfd_sq(P, Q)), (rows, skew, n1, n2, d)
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("k", [2, 8, 64])
+def test_coarse_upper_bound(ctx, built, k):
+    """rfd_options.coarse_ub: a certified upper bound in place of the DFD.  VE-FD is pruned by
+    it exactly (bit-identical), the FD agrees within the stop rule, and the bound is >= DFD."""
+    cases = [built.gen_pair(1, 3, 3000, 2800, 100.0, 0.1, 61, 0),
+             built.gen_pair(0, 2, 900, 850, 1.0, 0.05, 61, 1),
+             built.gen_pair(1, 2, 257, 4000, 100.0, 0.1, 61, 2),
+             (np.array([[0.5, 0.5]]), built.gen_pair(0, 2, 50, 60, 1.0, 0.05, 61, 3)[1])]
+    tol = 2.0 ** -33
+    for n, (P, Q) in enumerate(cases):
+        a = ctx.distance(P, Q, precise=True)
+        b = ctx.distance(P, Q, precise=True, coarse_ub=k)
+        assert b["vefd"] == a["vefd"], n
+        assert abs(b["distance"] - a["distance"]) <= 2 * tol * a["distance"], n
+        if len(P) >= 2 and len(Q) >= 2:
+            assert b["flags"] & built.FLAG_DFD_COARSE and b["dfd"] >= a["dfd"], n
+        else:  # a one-point curve keeps the exact DFD, its closed-form answer
+            assert b["distance"] == a["distance"] and not (b["flags"] & built.FLAG_DFD_COARSE)
+    Ps, Qs = [c[0] for c in cases], [c[1] for c in cases]
+    got = ctx.distance_batch(Ps, Qs, precise=True, coarse_ub=k, model=built.Model.pretrained(0))
+    for n, (P, Q) in enumerate(cases):
+        want = ctx.distance(P, Q, precise=True)["distance"]
+        assert abs(got[n]["distance"] - want) <= 2 * tol * want, n
+
+
+def test_coarse_upper_bound_checked(ctx, built):
+    P, Q = built.gen_pair(0, 2, 100, 90, 1.0, 0.05, 61, 4)
+    for bad in (dict(coarse_ub=1), dict(coarse_ub=-3), dict(coarse_ub=8, precise=False)):
+        with pytest.raises(built.RfdError):
+            ctx.distance(P, Q, **bad)
