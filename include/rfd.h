@@ -145,6 +145,17 @@ int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const
                            const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
                            const int32_t* dims, const rfd_options* opt, rfd_result* out);
 
+/* All pairwise distances of ncurves curves (no reference counterpart: the many-to-many use of
+   the reference's Curves, include/curve.hpp:42-47).  out is ncurves x ncurves, row-major,
+   symmetric with a zero diagonal; entry (i, j), i < j, is the distance with curve i as the
+   first curve.  results (optional) receives the ncurves (ncurves - 1) / 2 pair results in
+   that order.  Pairs go through rfd_distance_batch in chunks whose strip boundary rows
+   (n_i n_j / 4 bytes a pair) stay within budget_bytes (<= 0: 8e9).  opt->bracket must be NULL;
+   the curves of a pair must have equal dims. */
+int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* const* curves,
+                            const int64_t* ns, const int32_t* dims, const rfd_options* opt,
+                            double budget_bytes, double* out, rfd_result* results);
+
 /* The two bounds.  *vefd is read as the endpoint lower bound that seeds VE-FD and
    overwritten with VE-FD (left unchanged when the reference rule skips it and
    reference_quirks != 0).  Replaces Cuda_intersection::Bound_call_gpu
@@ -213,6 +224,15 @@ int32_t rfd_features(rfd_context* ctx, int64_t npairs, const double* const* c1s,
    malloc'd [*n][dims] array released with rfd_free. */
 int32_t rfd_load_txt(const char* path, int32_t dims, int32_t start, int32_t limit, double** out,
                      int64_t* n);
+
+/* rfd_load_txt with the parsing spread over `threads` host threads (<= 0: all cores); the
+   same rules and results (no reference counterpart: the survey's fast loader). */
+int32_t rfd_load_txt_fast(const char* path, int32_t dims, int32_t start, int32_t limit,
+                          int32_t threads, double** out, int64_t* n);
+/* Binary trajectory files: "RFDB", uint32 version 1, int32 dims, int32 0, int64 n, then n*dims
+   little-endian doubles.  rfd_load_bin's *out is freed with rfd_free. */
+int32_t rfd_save_bin(const char* path, const double* pts, int64_t n, int32_t dims);
+int32_t rfd_load_bin(const char* path, double** out, int64_t* n, int32_t* dims);
 void rfd_free(void* p);
 
 /* ---- synthetic workloads (seeded; see robotfd_b200/csrc/rfd_gen.cpp) ---- */

@@ -8,3 +8,9 @@
 #include "frechet.hpp"
 
 double compute_distance_parallel(const Curve& curve1, const Curve& curve2, bool forceOversize = false);
+
+// All pairwise distances of a Curves collection (no counterpart in the reference), row-major
+// n x n, symmetric with a zero diagonal; precise selects the 2^-33 relative stop rule instead
+// of the reference's FLT_EPSILON absolute one.
+#include <vector>
+std::vector<double> compute_distance_matrix(const Curves& curves, bool precise = false);

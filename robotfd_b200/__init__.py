@@ -55,7 +55,8 @@ EXPORTS = (
     "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
     "rfd_model_num_params", "rfd_model_create", "rfd_model_destroy", "rfd_model_set_params",
     "rfd_model_get_params", "rfd_model_forward", "rfd_model_gradients", "rfd_model_train_step",
-    "rfd_features", "rfd_gemm_bf16", "rfd_interval_class",
+    "rfd_features", "rfd_gemm_bf16", "rfd_interval_class", "rfd_distance_matrix",
+    "rfd_load_txt_fast", "rfd_save_bin", "rfd_load_bin",
 )
 
 
@@ -148,6 +149,12 @@ def lib():
     L.rfd_decide.restype = i32
     L.rfd_load_txt.argtypes = [ctypes.c_char_p, i32, i32, i32, ctypes.POINTER(_dp), _i64p]
     L.rfd_load_txt.restype = i32
+    L.rfd_load_txt_fast.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, ctypes.POINTER(_dp), _i64p]
+    L.rfd_load_txt_fast.restype = i32
+    L.rfd_save_bin.argtypes = [ctypes.c_char_p, _dp, i64, i32]
+    L.rfd_save_bin.restype = i32
+    L.rfd_load_bin.argtypes = [ctypes.c_char_p, ctypes.POINTER(_dp), _i64p, _i32p]
+    L.rfd_load_bin.restype = i32
     L.rfd_free.argtypes = [vp]
     L.rfd_free.restype = None
     L.rfd_gen_pair.argtypes = [i32, i32, i64, i64, dbl, dbl, ctypes.c_uint64, ctypes.c_uint64,
@@ -159,6 +166,8 @@ def lib():
     L.rfd_search_step.restype = i32
     L.rfd_interval_class.argtypes = [i64, _dp, _dp, _dp, _dp, dbl, i32, _i32p]
     L.rfd_interval_class.restype = i32
+    L.rfd_distance_matrix.argtypes = [vp, i64, vp, _i64p, _i32p, vp, dbl, _dp, vp]
+    L.rfd_distance_matrix.restype = i32
     L.rfd_decide_noalloc.argtypes = [vp, i64, vp, i64, i32, dbl, vp, vp]
     L.rfd_decide_noalloc.restype = i32
     fp = ctypes.POINTER(ctypes.c_float)
@@ -314,6 +323,11 @@ class Context:
         return bool(reach.value), rub.value
 
     # ---- batch
+    def distance_matrix(self, curves, budget_bytes=0.0, with_results=False, **kw):
+        """All pairwise distances (rfd_distance_matrix): an (n, n) array, symmetric, zero
+        diagonal; with with_results also the list of pair results (i < j, row-major)."""
+        return _matrix(self, curves, budget_bytes, with_results, **kw)
+
     def distance_batch(self, Ps, Qs, brackets=None, **kw):
         """Ps, Qs: sequences of host arrays, or (with memory=RFD_MEM_DEVICE) of
         (device_pointer, n, dims) tuples."""
@@ -344,6 +358,20 @@ class Context:
         return [r.as_dict() for r in res]
 
 
+def _matrix(ctx, curves, budget_bytes=0.0, with_results=False, **kw):
+    cs = [_curve(c) for c in curves]
+    n = len(cs)
+    ptrs = (ctypes.c_void_p * n)(*[c.ctypes.data for c in cs])
+    ns = (ctypes.c_int64 * n)(*[len(c) for c in cs])
+    dm = (ctypes.c_int32 * n)(*[c.shape[1] for c in cs])
+    o = options(**kw)
+    out = np.empty((n, n))
+    res = (Result * (n * (n - 1) // 2))() if with_results else None
+    _check(lib().rfd_distance_matrix(ctx._h, n, ptrs, ns, dm, ctypes.byref(o), float(budget_bytes),
+                                     out.ctypes.data_as(_dp), res))
+    return (out, [r.as_dict() for r in res]) if with_results else out
+
+
 def _endpoint_host(P, Q):
     a = float(np.sum((P[0] - Q[0]) ** 2))
     b = float(np.sum((P[-1] - Q[-1]) ** 2))
@@ -367,11 +395,15 @@ def compute_distance_parallel(curve1, curve2, force_oversize=False):
     return default_context().distance(curve1, curve2)["distance"]
 
 
-def _load(path, dims, start, limit):
+def _load(path, dims, start, limit, threads=None):
     out = _dp()
     n = ctypes.c_int64()
-    _check(lib().rfd_load_txt(str(path).encode(), dims, int(start), int(limit), ctypes.byref(out),
-                              ctypes.byref(n)))
+    if threads is None:
+        _check(lib().rfd_load_txt(str(path).encode(), dims, int(start), int(limit),
+                                  ctypes.byref(out), ctypes.byref(n)))
+    else:
+        _check(lib().rfd_load_txt_fast(str(path).encode(), dims, int(start), int(limit),
+                                       int(threads), ctypes.byref(out), ctypes.byref(n)))
     try:
         arr = np.ctypeslib.as_array(out, shape=(n.value * dims,)).copy() if n.value else np.zeros(0)
     finally:
@@ -387,6 +419,33 @@ def txt_loader2(path, start=0, limit=10000000):
 def txt_loader3(path, start=0, limit=10000000):
     """txtLoader3 (include/txtReader.hpp:48 of the reference) as an (n, 3) array."""
     return _load(path, 3, start, limit)
+
+
+def txt_loader_fast(path, dims, start=0, limit=10000000, threads=0):
+    """rfd_load_txt_fast: the loaders' rules with the parsing on `threads` host threads
+    (0: all cores)."""
+    return _load(path, dims, start, limit, threads)
+
+
+def save_bin(path, pts):
+    """Writes a curve as a binary trajectory file (rfd_save_bin)."""
+    a = np.ascontiguousarray(pts, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError("a curve is an (n, dims) array")
+    _check(lib().rfd_save_bin(str(path).encode(), a.ctypes.data_as(_dp), a.shape[0], a.shape[1]))
+
+
+def load_bin(path):
+    """Reads a binary trajectory file (rfd_load_bin) as an (n, dims) array."""
+    out = _dp()
+    n = ctypes.c_int64()
+    d = ctypes.c_int32()
+    _check(lib().rfd_load_bin(str(path).encode(), ctypes.byref(out), ctypes.byref(n), ctypes.byref(d)))
+    try:
+        arr = np.ctypeslib.as_array(out, shape=(n.value * d.value,)).copy() if n.value else np.zeros(0)
+    finally:
+        lib().rfd_free(out)
+    return arr.reshape(n.value, d.value)
 
 
 # ---- synthetic workloads

@@ -1209,6 +1209,58 @@ int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const
   return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
 }
 
+int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* const* curves,
+                            const int64_t* ns, const int32_t* dims, const rfd_options* opt,
+                            double budget_bytes, double* out, rfd_result* results) {
+  if (!ctx || !curves || !ns || !dims || !out || ncurves < 1)
+    return fail(RFD_ERR_ARG, "distance_matrix arguments");
+  if (ncurves > (1 << 20)) return fail(RFD_ERR_LIMIT, "more than 2^20 curves");
+  if (opt && opt->bracket) return fail(RFD_ERR_ARG, "distance_matrix takes no per-pair bracket");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  // pairs (i, j), i < j, go to the batch engine in chunks whose strip boundary rows (n1 n2 / 4
+  // bytes a pair, the bulk of the workspace) stay within the budget
+  const double budget = budget_bytes > 0.0 ? budget_bytes : 8e9;
+  const int64_t N = ncurves;
+  std::vector<const double*> c1, c2;
+  std::vector<int64_t> n1, n2, where;
+  std::vector<int32_t> dm;
+  std::vector<rfd_result> res;
+  double acc = 0.0;
+  auto flush = [&]() -> int {
+    if (where.empty()) return RFD_OK;
+    res.resize(where.size());
+    const int rc = run_batch(ctx, (int64_t)where.size(), c1.data(), n1.data(), c2.data(), n2.data(),
+                             dm.data(), opt, res.data(), MODE_DISTANCE, 0.0);
+    if (rc) return rc;
+    for (size_t k = 0; k < where.size(); ++k) {
+      const int64_t i = where[k] / N, j = where[k] % N;
+      out[i * N + j] = out[j * N + i] = res[k].distance;
+      if (results) results[i * N - i * (i + 1) / 2 + (j - i - 1)] = res[k];
+    }
+    c1.clear(); c2.clear(); n1.clear(); n2.clear(); dm.clear(); where.clear();
+    acc = 0.0;
+    return RFD_OK;
+  };
+  for (int64_t i = 0; i < N; ++i) out[i * N + i] = 0.0;
+  for (int64_t i = 0; i < N; ++i)
+    for (int64_t j = i + 1; j < N; ++j) {
+      if (dims[i] != dims[j]) return fail(RFD_ERR_ARG, "curves of a pair differ in dimension");
+      const double bytes = (double)ns[i] * (double)ns[j] / 4.0 + 256.0 * (double)(ns[i] + ns[j]);
+      if (acc + bytes > budget && !where.empty()) {
+        const int rc = flush();
+        if (rc) return rc;
+      }
+      c1.push_back(curves[i]);
+      c2.push_back(curves[j]);
+      n1.push_back(ns[i]);
+      n2.push_back(ns[j]);
+      dm.push_back(dims[i]);
+      where.push_back(i * N + j);
+      acc += bytes;
+    }
+  return flush();
+}
+
 int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
                    int32_t dims, int32_t reference_quirks, int32_t dense, double* dfd, double* vefd) {
   if (!ctx || !dfd || !vefd) return fail(RFD_ERR_ARG, "null argument");

@@ -235,3 +235,10 @@ def test_cpp_headers_compile_and_load(built, tmp_path):
 def test_cli_usage(built):
     r = subprocess.run([built.FD_PATH], capture_output=True, text=True)
     assert r.returncode == 1 and "Usage" in r.stderr
+
+
+def test_distance_matrix_checks_arguments_without_a_context(built):
+    """The matrix entry point validates its arguments before touching a device."""
+    import ctypes
+    rc = built.lib().rfd_distance_matrix(None, 2, None, None, None, None, 0.0, None, None)
+    assert rc == built.RFD_ERR_ARG
