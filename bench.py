@@ -203,12 +203,29 @@ def batch_pairs(npairs=4096, seed=2):
         return list(ex.map(one, range(npairs)))
 
 
-def batch_leg(ctx, model, timed, sample=128):
+def batch_leg(ctx, model, timed, sample=128, dist=None):
     """4096 uneven pairs: learned batched, plain batched, and plain single-pair calls on a
-    fixed sample (every 32nd pair), each timed with CUDA events on the context stream."""
+    fixed sample (every 32nd pair), each timed with CUDA events on the context stream.  Under
+    torchrun the learned batch is sharded over the ranks (robotfd_b200.shard: a fixed 4096
+    pairs, strong scaling), timed as the maximum over ranks."""
     pairs = batch_pairs()
     Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
     n = len(Ps)
+    if dist is not None:
+        import torch
+        from robotfd_b200 import shard
+        shard.distance_batch_sharded(ctx, Ps[:256], Qs[:256], precise=True, model=model)  # warm
+        t_s, res = timed(lambda: shard.distance_batch_sharded(ctx, Ps, Qs, precise=True,
+                                                              model=model), 2)
+        t = torch.tensor([statistics.median(t_s)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return {
+            "workload": "4096 uneven pairs (config 2 generator, seed 2), sharded over "
+                        f"{dist.get_world_size()} ranks by cells; FD to 2^-33 relative",
+            "solves_per_s": {"learned_sharded": n / (float(t.item()) * 1e-3)},
+            "scaling": "strong (the 4096 pairs are split over the ranks)",
+            "mean_probes": {"learned": statistics.mean(r["probes"] for r in res)},
+        }
     ctx.distance_batch(Ps[:64], Qs[:64], precise=True, model=model)  # warm
     t_l, learned = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model), 2)
     t_c, _ = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
@@ -452,8 +469,8 @@ def main():
         "clocks": clk,
     }
     if not args.no_batch:
-        line["batch"] = batch_leg(ctx, model, timed)
-    if args.mixed_pairs > 0:
+        line["batch"] = batch_leg(ctx, model, timed, dist=dist)
+    if args.mixed_pairs > 0 and world == 1:
         line["mixed_precision"] = mixed_leg(ctx, model, timed, args.mixed_pairs)
     if rank == 0:
         if world == 1:
