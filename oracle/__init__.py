@@ -7,6 +7,10 @@ reference's DFD, VE-FD and fused-decision cells and its epsilon search (file:lin
 citations in its header).  Its search driver, endpoint bound and the loaders are pinned by
 the reference's own host code run on the same inputs (``tests/golden``); its cells by
 mathematical known-answer tests and brute-force definitions (``tests/test_oracle.py``).
+
+``verify.c`` is a separate, formula-independent checker: it decides reachability at a radius
+in exact real arithmetic on the given doubles (certified inner and outer free intervals), or
+says that it cannot tell (``tests/test_verify.py``).
 """
 import ctypes
 import os
@@ -48,6 +52,9 @@ def lib():
                                         ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_int, _dp, _ip]
         L.rfd_oracle_max_threads.restype = ctypes.c_int
+        L.rfd_verify_decision.restype = ctypes.c_int
+        L.rfd_verify_decision.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double]
+        L.rfd_verify_free_bounds.argtypes = [_dp, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp]
         L.rfd_oracle_free_intervals.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, ctypes.c_double,
                                                 ctypes.c_int, _dp, _dp]
         _LIB = L
@@ -158,3 +165,21 @@ def free_intervals(x, a, b, A, r2):
     if rc:
         raise RuntimeError("oracle free_intervals failed")
     return lo, hi
+
+
+def verify_decision(P, Q, radius):
+    """+1 if the free space at `radius` is certainly traversable, -1 if certainly not, 0 if
+    the verifier cannot tell (exact real arithmetic on the given doubles)."""
+    P, Q = _arr(P), _arr(Q)
+    if P.shape[1] != Q.shape[1]:
+        raise ValueError("curves differ in dimension")
+    return lib().rfd_verify_decision(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], float(radius))
+
+
+def verify_free_bounds(x, s, e, radius):
+    """(inner, outer) bounds of the free interval of segment s -> e around x; each a (lo, hi)
+    pair, empty when lo > hi."""
+    x, s, e = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, s, e))
+    out = (ctypes.c_double * 4)()
+    lib().rfd_verify_free_bounds(_ptr(x), _ptr(s), _ptr(e), float(radius), len(x), out)
+    return (out[0], out[1]), (out[2], out[3])

@@ -1,0 +1,110 @@
+"""GPU results certified by the exact decision verifier (oracle/verify.c).
+
+Every bracket [lb, ub] the engine returns -- single pairs, the batch with the learned bracket,
+the FP32 filter and the coarse upper bound -- contains the exact Frechet distance, and the
+GPU's decisions around the distance agree with the exact ones, both up to the rounding of
+the reference's FP64 formulas.  That rounding is bounded per pair by the conditioning
+slack below: the free-interval discriminant B^2 - 4AC loses about eps |x - a|^2 to
+cancellation, so the radius at which an edge opens moves by about eps (|x - a| / r)^2
+relatively, |x - a| at most the diameter of the two curves.
+
+Curves with consecutive repeated points are excluded here: the reference's free interval of
+a zero-length segment is [0, 1] at every radius (0 * inf = NaN, clamped by fmax / fmin), so
+its decisions, which the engine reproduces, are not the exact ones for them
+(test_repeated_points_follow_the_reference)."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+ULP = 2.0 ** -52
+
+
+def pairs(built):
+    out = [built.gen_pair(k % 2, 2 + k % 2, 60 + 45 * k, 90 + 30 * k, 10.0 ** (k % 4 - 1), 0.05,
+                          31, k) for k in range(10)]
+    rng = np.random.default_rng(9)
+    for k in range(6):  # random walks, one of them against a one-point curve
+        P = np.cumsum(rng.normal(size=(int(rng.integers(2, 300)), 2)), 0)
+        Q = np.cumsum(rng.normal(size=(int(rng.integers(2, 300)), 2)), 0)
+        out.append((P[:1] if k == 0 else P, Q))
+    return out
+
+
+def slack(P, Q, r):
+    """Relative rounding slack of the FP64 decision at radius r (see the module docstring)."""
+    both = np.concatenate([P, Q])
+    diam = float(np.linalg.norm(both.max(0) - both.min(0)))
+    return 8 * ULP * max(1.0, (diam / r) ** 2)
+
+
+def certify(P, Q, res):
+    lb, ub = res["lb"], res["ub"]
+    assert lb <= res["distance"] <= ub
+    assert oracle.verify_decision(P, Q, ub * (1 + slack(P, Q, ub))) == 1, res
+    assert oracle.verify_decision(P, Q, lb * (1 - slack(P, Q, lb))) == -1, res
+
+
+@pytest.mark.parametrize("precise", [True, False])
+def test_single_pair_brackets_contain_exact_distance(ctx, built, precise):
+    for P, Q in pairs(built):
+        certify(P, Q, ctx.distance(P, Q, precise=precise))
+
+
+def test_batch_brackets_contain_exact_distance(ctx, built):
+    ps = pairs(built)
+    Ps, Qs = [p for p, _ in ps], [q for _, q in ps]
+    model = built.Model.pretrained(0)
+    for kw in ({}, {"model": model}, {"precision": built.RFD_PREC_FP32_FILTER},
+               {"coarse_ub": 4}, {"model": model, "coarse_ub": 4}):
+        for (P, Q), res in zip(ps, ctx.distance_batch(Ps, Qs, precise=True, **kw)):
+            certify(P, Q, res)
+
+
+def flip(decide, lo, hi):
+    """The smallest double in (lo, hi] at which decide() holds (decide(lo) false, hi true)."""
+    a, b = lo, hi
+    while True:
+        m = 0.5 * (a + b)
+        if m <= a or m >= b:
+            return b
+        if decide(m):
+            b = m
+        else:
+            a = m
+
+
+def test_gpu_decisions_near_the_threshold(ctx, built):
+    """The exact threshold is pinned to the verifier's band [r_lo, r_hi]; outside that band,
+    widened by the rounding slack, the GPU decides exactly."""
+    tight = 0
+    for P, Q in pairs(built)[:8]:
+        fd = ctx.distance(P, Q, precise=True)["distance"]
+        lo, hi = fd * 0.9, fd * 1.1
+        r_hi = flip(lambda r: oracle.verify_decision(P, Q, r) == 1, lo, hi)
+        r_lo = flip(lambda r: oracle.verify_decision(P, Q, r) != -1, lo, hi)
+        w = slack(P, Q, fd)
+        assert r_hi - r_lo <= w * fd
+        tight += w <= 1e-12
+        for k in (0, 1, 4, 64, 1 << 20):
+            assert not ctx.decide(P, Q, r_lo * (1 - w) - k * ULP * fd)[0], k
+            assert ctx.decide(P, Q, r_hi * (1 + w) + k * ULP * fd)[0], k
+    assert tight >= 4
+
+
+def test_repeated_points_follow_the_reference(ctx, built):
+    """A repeated point: the peak of height 3 is missed by the reference's decision (its
+    zero-length segment is free at every radius), and the engine reproduces that; without the
+    repeat (the same curve, the same exact distance) both decide exactly."""
+    P = np.array([[0.0, 0], [1, 0], [1, 0], [2, 0]])
+    Q = np.array([[0.0, 0], [1, 3], [2, 0]])
+    for r in (1.0, 2.0, 2.9):
+        assert oracle.verify_decision(P, Q, r) == -1
+        assert oracle.decide(P, Q, r)[0] and ctx.decide(P, Q, r)[0]
+        assert not ctx.decide(P[[0, 1, 3]], Q, r)[0]
+    got = ctx.distance(P, Q, precise=True)
+    assert got["distance"] == oracle.distance(P, Q, stop_mode=1)["distance"] < 1.0
+    exact = ctx.distance(P[[0, 1, 3]], Q, precise=True)
+    certify(P, Q, exact)
