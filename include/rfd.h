@@ -83,6 +83,14 @@ typedef struct rfd_options {
                                the DFD from k*k times fewer cells.  result.dfd then holds that
                                bound (RFD_FLAG_DFD_COARSE).  The FD, within the stop rule, does
                                not depend on it. */
+  int32_t drop_repeats;     /* 1: drop consecutive repeated points (all coordinates equal) from
+                               both curves before the solve (host memory only).  The Frechet
+                               distance does not change in exact arithmetic, but the reference's
+                               free interval of a zero-length segment is [0, 1] at every radius
+                               (src/intersection_algorithm_in_parallel.cu:1186-1198: 0 * inf is
+                               NaN, which max / min clamp to the whole edge), so a repeated point
+                               can make its decisions, and the distance, too small.  0 (default)
+                               keeps the reference's behaviour. */
 } rfd_options;
 
 typedef struct rfd_result {

@@ -78,6 +78,7 @@ class Options(ctypes.Structure):
         ("bracket", ctypes.POINTER(ctypes.c_double)),
         ("model", ctypes.c_void_p),
         ("coarse_ub", ctypes.c_int32),
+        ("drop_repeats", ctypes.c_int32),
     ]
 
 
@@ -215,7 +216,7 @@ def _curve(c):
 
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
-            precision=RFD_PREC_FP64, model=None, coarse_ub=0):
+            precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -229,6 +230,7 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
     if model is not None:
         o.model = model._h.value
     o.coarse_ub = int(coarse_ub)
+    o.drop_repeats = int(bool(drop_repeats))
     return o
 
 

@@ -593,6 +593,32 @@ int check_pair(const double* c1, int64_t n1, const double* c2, int64_t n2, int32
   return RFD_OK;
 }
 
+// Consecutive repeated points (rfd_options.drop_repeats): point k is kept unless every
+// coordinate equals point k-1's.  A zero-length segment is exactly the case A = 0 of the
+// free-interval quadratic, so the kept curve has none.
+static bool same_point(const double* a, const double* b, int d) {
+  for (int k = 0; k < d; ++k)
+    if (!(a[k] == b[k])) return false;
+  return true;
+}
+
+static int64_t kept_points(const double* c, int64_t n, int d) {
+  int64_t m = n > 0 ? 1 : 0;
+  for (int64_t k = 1; k < n; ++k) m += !same_point(c + (k - 1) * d, c + k * d, d);
+  return m;
+}
+
+static void copy_kept(double* dst, const double* c, int64_t n, int d) {
+  if (n < 1) return;
+  memcpy(dst, c, sizeof(double) * d);
+  double* last = dst;
+  for (int64_t k = 1; k < n; ++k) {
+    if (same_point(c + (k - 1) * d, c + k * d, d)) continue;
+    last += d;
+    memcpy(last, c + k * d, sizeof(double) * d);
+  }
+}
+
 int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
               const double* const* c2s, const int64_t* n2s, const int32_t* dims,
               const rfd_options* opt, rfd_result* out, int mode, double radius) {
@@ -620,6 +646,23 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   }
   const bool on_device = o.memory == RFD_MEM_DEVICE;
   const int max_probes = mode == MODE_DISTANCE ? o.max_probes : 0;
+  if (o.drop_repeats != 0 && o.drop_repeats != 1) return fail(RFD_ERR_ARG, "drop_repeats");
+  // with drop_repeats the layout is sized by the kept points; the staging copy compacts
+  const int64_t* const in_n1s = n1s;
+  const int64_t* const in_n2s = n2s;
+  std::vector<int64_t> kept1, kept2;
+  const bool drop = mode == MODE_DISTANCE && o.drop_repeats;
+  if (drop) {
+    if (on_device) return fail(RFD_ERR_ARG, "drop_repeats needs curves in host memory");
+    kept1.resize(npairs);
+    kept2.resize(npairs);
+    for (int64_t p = 0; p < npairs; ++p) {
+      kept1[p] = kept_points(c1s[p], n1s[p], dims[p]);
+      kept2[p] = kept_points(c2s[p], n2s[p], dims[p]);
+    }
+    n1s = kept1.data();
+    n2s = kept2.data();
+  }
 
   // ---------------- layout
   Layout L;
@@ -725,6 +768,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     if (on_device) {
       D.P = c1s[p];
       D.Q = c2s[p];
+    } else if (drop) {
+      copy_kept((double*)(hbase + L.hP[p]), c1s[p], in_n1s[p], d);
+      copy_kept((double*)(hbase + L.hQ[p]), c2s[p], in_n2s[p], d);
+      D.P = (const double*)(dbase + L.P[p]);
+      D.Q = (const double*)(dbase + L.Q[p]);
     } else {
       memcpy(hbase + L.hP[p], c1s[p], sizeof(double) * n1 * d);
       memcpy(hbase + L.hQ[p], c2s[p], sizeof(double) * n2 * d);

@@ -97,14 +97,69 @@ def test_gpu_decisions_near_the_threshold(ctx, built):
 def test_repeated_points_follow_the_reference(ctx, built):
     """A repeated point: the peak of height 3 is missed by the reference's decision (its
     zero-length segment is free at every radius), and the engine reproduces that; without the
-    repeat (the same curve, the same exact distance) both decide exactly."""
+    repeat (the same curve, the same exact distance) both decide exactly.  The reference's own
+    method (no VE-FD for pairs of at most 10000 cells) searches up from the endpoint bound and
+    lands below 1; a VE-FD lower bound (precise mode) happens to hide it on this pair."""
     P = np.array([[0.0, 0], [1, 0], [1, 0], [2, 0]])
     Q = np.array([[0.0, 0], [1, 3], [2, 0]])
     for r in (1.0, 2.0, 2.9):
         assert oracle.verify_decision(P, Q, r) == -1
         assert oracle.decide(P, Q, r)[0] and ctx.decide(P, Q, r)[0]
         assert not ctx.decide(P[[0, 1, 3]], Q, r)[0]
-    got = ctx.distance(P, Q, precise=True)
-    assert got["distance"] == oracle.distance(P, Q, stop_mode=1)["distance"] < 1.0
-    exact = ctx.distance(P[[0, 1, 3]], Q, precise=True)
-    certify(P, Q, exact)
+    got = ctx.distance(P, Q)
+    assert got["distance"] == oracle.distance(P, Q)["distance"] < 1.0
+    certify(P, Q, ctx.distance(P[[0, 1, 3]], Q))
+
+
+def without_repeats(P):
+    keep = np.concatenate([[True], np.any(P[1:] != P[:-1], axis=1)])
+    return P[keep]
+
+
+def with_repeats(rng, P):
+    """P with runs of repeated points (a trajectory's stationary periods)."""
+    reps = rng.integers(1, 4, size=len(P)) * (rng.random(len(P)) < 0.2) + 1
+    return np.repeat(P, reps, axis=0)
+
+
+def test_drop_repeats_gives_the_exact_distance(ctx, built):
+    P = np.array([[0.0, 0], [1, 0], [1, 0], [2, 0]])
+    Q = np.array([[0.0, 0], [1, 3], [2, 0]])
+    for precise in (False, True):
+        a = ctx.distance(P, Q, precise=precise, drop_repeats=True)
+        b = ctx.distance(P[[0, 1, 3]], Q, precise=precise)
+        for key in ("distance", "lb", "ub", "dfd", "vefd", "endpoint", "probes", "cells_nominal"):
+            assert a[key] == b[key], key
+        certify(P, Q, a)
+        assert abs(a["distance"] - 3.0) <= 1e-6
+
+
+def test_drop_repeats_batch(ctx, built):
+    rng = np.random.default_rng(4)
+    ps = []
+    for k in range(12):
+        d = 2 + k % 2
+        P = with_repeats(rng, np.cumsum(rng.normal(size=(int(rng.integers(2, 250)), d)), 0))
+        Q = with_repeats(rng, np.cumsum(rng.normal(size=(int(rng.integers(2, 250)), d)), 0))
+        ps.append((P, Q))
+    ps.append((np.repeat([[1.0, 2.0]], 5, axis=0), ps[0][1]))  # a curve of one repeated point
+    Ps, Qs = [p for p, _ in ps], [q for _, q in ps]
+    for precise in (False, True):
+        got = ctx.distance_batch(Ps, Qs, precise=precise, drop_repeats=True)
+        want = ctx.distance_batch([without_repeats(p) for p in Ps],
+                                  [without_repeats(q) for q in Qs], precise=precise)
+        for (P, Q), a, b in zip(ps, got, want):
+            for key in ("distance", "lb", "ub", "dfd", "vefd", "probes", "cells_nominal"):
+                assert a[key] == b[key], key
+            certify(P, Q, a)
+        if not precise:
+            # the reference's behaviour is kept by default: some pair comes out too small
+            plain = ctx.distance_batch(Ps, Qs)
+            assert any(a["distance"] < b["distance"] for a, b in zip(plain, got))
+
+
+def test_drop_repeats_needs_host_curves(ctx, built):
+    import torch
+    P = torch.zeros((4, 2), dtype=torch.float64, device="cuda")
+    with pytest.raises(built.RfdError):
+        ctx.distance_device(P.data_ptr(), 4, P.data_ptr(), 4, 2, drop_repeats=True)
