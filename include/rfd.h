@@ -89,8 +89,10 @@ typedef struct rfd_options {
                                free interval of a zero-length segment is [0, 1] at every radius
                                (src/intersection_algorithm_in_parallel.cu:1186-1198: 0 * inf is
                                NaN, which max / min clamp to the whole edge), so a repeated point
-                               can make its decisions, and the distance, too small.  0 (default)
-                               keeps the reference's behaviour. */
+                               can make its decisions, and the distance, too small.  The
+                               reference's text loaders drop such points (include/txtReader.hpp:
+                               36-41); this applies the same rule to curves built in code.
+                               0 (default) keeps the reference's behaviour. */
 } rfd_options;
 
 typedef struct rfd_result {
