@@ -242,3 +242,31 @@ def test_distance_matrix_checks_arguments_without_a_context(built):
     import ctypes
     rc = built.lib().rfd_distance_matrix(None, 2, None, None, None, None, 0.0, None, None)
     assert rc == built.RFD_ERR_ARG
+
+
+def test_ctypes_structs_match_the_header(built, tmp_path):
+    """The Python mirrors of rfd_options and rfd_result have the C layout (size and offsets)."""
+    fields = {"rfd_options": (built.Options, [f for f, _ in built.Options._fields_]),
+              "rfd_result": (built.Result, [f for f, _ in built.Result._fields_])}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "rfd.h"', "int main(void) {"]
+    for name, (_, names) in fields.items():
+        lines.append(f'  printf("%zu\\n", sizeof({name}));')
+        lines += [f'  printf("%zu\\n", offsetof({name}, {f}));' for f in names]
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    want = []
+    for _, (cls, names) in fields.items():
+        want.append(ctypes_sizeof(cls))
+        want += [getattr(cls, f).offset for f in names]
+    assert got == want
+
+
+def ctypes_sizeof(cls):
+    import ctypes
+    return ctypes.sizeof(cls)
