@@ -318,16 +318,18 @@ template <int KIND>
 __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   extern __shared__ __align__(128) unsigned char team_smem[];
   TeamShared* sh = (TeamShared*)team_smem;
-  double2* tiles = (double2*)(team_smem + 256);
+  double2* tiles = (double2*)(team_smem + kTeamHeader);
+  double* stage = (double*)(team_smem + kTeamHeader + 2 * TileT<KIND>::slot_bytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int k = 0; k < 2; ++k) {
       mbar_init(&sh->full[k], kHelpers);
       mbar_init(&sh->req[k], 1);
     }
+    mbar_init(&sh->staged, kHelpers);
   }
   __syncthreads();
-  unsigned seqP = 0, seqC = 0, seqH = 0;
+  unsigned seqP = 0, seqC = 0, seqH = 0, seqS = 0;
   for (;;) {
     if (threadIdx.x == 0) {
       int go = 0, quit = 0;
@@ -366,8 +368,8 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
                                    : team_propagator<KIND, 3>(wa, pd, st, s, sh, tiles, seqP, seqC);
       if (lane == 0) sh->status = status;
     } else {
-      if (pd.d == 2) team_helpers<KIND, 2>(wa, pd, st, s, sh, tiles, seqH, warp - 1);
-      else team_helpers<KIND, 3>(wa, pd, st, s, sh, tiles, seqH, warp - 1);
+      if (pd.d == 2) team_helpers<KIND, 2>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
+      else team_helpers<KIND, 3>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
     }
     __syncthreads();
     if (threadIdx.x == 0 && sh->status == 0) {

@@ -26,6 +26,7 @@ constexpr int kStop = -2;  // request word: strip finished
 struct TeamShared {
   unsigned long long full[2];  // helpers -> propagator: tile ready (kHelpers arrivals)
   unsigned long long req[2];   // propagator -> helpers: chunk requested (1 arrival)
+  unsigned long long staged;   // helpers -> helpers: a tile's column records are staged
   int req_chunk[2];
   int cancel[2];
   int item_pair, item_strip, go, quit;
@@ -33,7 +34,19 @@ struct TeamShared {
   unsigned long long evaluated64;  // of those, cells with an interval computed in FP64
   int status;
   int pad;
+  // the strip's last row, two 32-column chunks: lane 31 stores each value as it is produced
+  // (off the propagation chain), the flush reads a chunk back one column per lane
+  double out_row[64];
 };
+
+// Column records of one tile, staged by the helpers: the tile of step-chunk c reads the
+// columns c*32-31 .. c*32+31, i.e. the points q_{c*32-31} .. q_{c*32+32} and the segments'
+// A and 0.5/A, as structure-of-arrays rows of 64 (conflict-free reads along a warp).
+constexpr int kStageRow = 64;
+constexpr int kStageDoubles = 5 * kStageRow;  // q[3][64], A[64], inv2A[64]
+
+constexpr size_t kTeamHeader = 1024;
+static_assert(sizeof(TeamShared) <= kTeamHeader, "team header");
 
 template <int KIND>
 struct TileT {
@@ -43,7 +56,7 @@ struct TileT {
 
 template <int KIND>
 __host__ __device__ constexpr size_t team_smem_bytes() {
-  return 256 + 2 * TileT<KIND>::slot_bytes;
+  return kTeamHeader + 2 * TileT<KIND>::slot_bytes + 2 * kStageDoubles * sizeof(double);
 }
 
 // ------------------------------------------------------------------ mbarrier helpers
@@ -90,7 +103,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
 
 template <int KIND, int D>
 __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairState* st, int s,
-                             TeamShared* sh, double2* tiles, unsigned& seqH, int hw) {
+                             TeamShared* sh, double2* tiles, double* stage, unsigned& seqH,
+                             unsigned& seqS, int hw) {
   const int lane = threadIdx.x & 31;
   const int R = pd.n1 - 1, C = pd.n2 - 1;
   const int i = (s << 5) + lane;
@@ -118,9 +132,44 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
     double2* T1 = T0 + 1024;
     const long long tc0 = wa.prof ? clock64() : 0;
-    // Two independent cells (u, u + kHelpers) per iteration, their records loaded with
-    // clamped indices so no load waits on a branch; results are stored only for cells
-    // inside the grid.
+    // Stage the tile's column records once for all helpers (one round of coalesced loads
+    // instead of a dependent load per cell pair), with clamped indices: a clamped record
+    // only feeds cells outside the grid, whose results are not stored.  Two buffers: a
+    // helper stages tile k+1 while slower ones may still read tile k.
+    double* buf = stage + (seqS & 1) * kStageDoubles;
+    {
+      const int base = (c << 5) - 31;
+      const int t = (hw << 5) + lane;
+      for (int e = t; e < kStageRow * D; e += 32 * kHelpers) {
+        const int jj = e / D, k = e - jj * D;
+        const int qi = min(max(base + jj, 0), C);
+        buf[k * kStageRow + jj] = __ldg(pd.Q + (size_t)qi * D + k);
+      }
+      constexpr int W = RecW<D>::value;
+      for (int e = t; e < kStageRow - 1; e += 32 * kHelpers) {
+        const int j = min(max(base + e, 0), C - 1);
+        const double2 a = __ldg(pd.colrec + (size_t)j * W + (W - 1));
+        buf[3 * kStageRow + e] = a.x;
+        buf[4 * kStageRow + e] = a.y;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sh->staged);
+    if (!mbar_wait(&sh->staged, seqS & 1, wa, t0)) break;
+    ++seqS;
+    // column j = c*32 + u - lane sits at jj = u - lane + 31 of the staged rows
+    auto col_at = [&](int u, ColRec<KIND, D>& col) {
+      const int jj = u - lane + 31;
+#pragma unroll
+      for (int k = 0; k < D; ++k) {
+        col.qa[k] = buf[k * kStageRow + jj];
+        col.qb[k] = buf[k * kStageRow + jj + 1];
+      }
+      col.A = buf[3 * kStageRow + jj];
+      col.inv2A = buf[4 * kStageRow + jj];
+    };
+    // Two independent cells (u, u + kHelpers) per iteration; results are stored only for
+    // cells inside the grid.
     auto one = [&](int u, const ColRec<KIND, D>& col) {
       const int j = (c << 5) + u - lane;
       double qd[D];
@@ -164,8 +213,8 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
       if (__shfl_sync(kFull, *(volatile int*)&sh->cancel[slot], 0)) break;
       const int u1 = u0 + kHelpers;
       ColRec<KIND, D> c0, c1;
-      load_col<KIND, D>(pd, min(max((c << 5) + u0 - lane, 0), C - 1), c0);
-      load_col<KIND, D>(pd, min(max((c << 5) + min(u1, 31) - lane, 0), C - 1), c1);
+      col_at(u0, c0);
+      col_at(min(u1, 31), c1);
       one(u0, c0);
       if (u1 < 32) one(u1, c1);
     }
@@ -245,7 +294,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   if (KIND == K_DEC) bot = i == 0 ? 0.0 : -1.0;
   else bot = i == 0 ? st->seed : kFltMax;
   double carry = dead_value<KIND>();
-  double ob0 = dead_value<KIND>(), ob1 = dead_value<KIND>();
+  double* out_row = sh->out_row;
+  out_row[lane] = dead_value<KIND>();
+  out_row[32 + lane] = dead_value<KIND>();
+  __syncwarp();
   unsigned first_live_out = kNone;
   int next_flush = 0;
   int pending = -1;  // chunk of the outstanding tile request (-1: none)
@@ -278,12 +330,12 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   };
   auto flush = [&](int k) {
     const int col = (k << 5) + lane;
-    double v = (k & 1) ? ob1 : ob0;
+    __syncwarp();
+    const double v = out_row[((k & 1) << 5) + lane];
     const bool valid = col < C;
     if (valid) st_relaxed_f64(out_bnd + col, v);
     const unsigned live = __ballot_sync(kFull, valid && !is_dead<KIND>(v, U));
-    if (k & 1) ob1 = dead_value<KIND>();
-    else ob0 = dead_value<KIND>();
+    out_row[((k & 1) << 5) + lane] = dead_value<KIND>();
     __syncwarp();
     if (lane == 0) {
       if (live) {
@@ -479,7 +531,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
           publish_cols(min((nc - 1) << 5, C));
         }
         carry = dead_value<KIND>();
-        ob0 = ob1 = dead_value<KIND>();
+        __syncwarp();
+        out_row[lane] = dead_value<KIND>();
+        out_row[32 + lane] = dead_value<KIND>();
+        __syncwarp();
         c = nc;
         if (pending != c) {
           request(c);  // cold start of the live stretch
@@ -538,11 +593,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       carry = act ? ncarry : carry;
       bot = act ? nbot : bot;
       if (act && last_row && j == C - 1) res = nres;
-      const double o = __shfl_sync(kFull, carry, 31);
-      if (lane == ((u + 1) & 31)) {  // lane 31 produced column (c << 5) + u - 31
-        if (((((c << 5) + u - 31) >> 5) & 1) != 0) ob1 = o;
-        else ob0 = o;
-      }
+      // lane 31 produced column (c << 5) + u - 31 of the strip's last row
+      if (lane == 31) out_row[((c << 5) + u - 31) & 63] = carry;
     }
     if (wa.prof && lane == 0) {
       atomicAdd(&wa.prof[3], (unsigned long long)(clock64() - ts0));
