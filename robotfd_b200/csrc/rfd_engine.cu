@@ -999,9 +999,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                         cudaMemcpyDeviceToHost));
     fprintf(stderr,
             "rfd prof (Mcycles): in_wait %.1f jump %.1f tile_wait %.1f steps %.1f strip_total %.1f |"
-            " chunks %llu jumps %llu strips %llu | helpers: tile %.1f req_wait %.1f tiles %llu\n",
+            " chunks %llu jumps %llu strips %llu | helpers: tile %.1f req_wait %.1f tiles %llu |"
+            " flush %.1f flushes %llu\n",
             pc[0] / 1e6, pc[1] / 1e6, pc[2] / 1e6, pc[3] / 1e6, pc[4] / 1e6, pc[5], pc[6], pc[7],
-            pc[8] / 1e6, pc[9] / 1e6, pc[10]);
+            pc[8] / 1e6, pc[9] / 1e6, pc[10], pc[11] / 1e6, pc[12]);
     // strip chain of the first pair: handoff = first live input of strip s after the first
     // live output of strip s-1; lag = first live output of strip s after its first live input
     std::vector<double> hand, lag, adv;

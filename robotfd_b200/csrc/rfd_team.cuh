@@ -328,7 +328,13 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     pending = -1;
     return take() >= 0;
   };
-  auto flush = [&](int k) {
+  // Flush of output chunk k: its words, then (lane 0) its tag and the first/last live hints.
+  // The progress word is released (after a fence) only when `publish` is set: the next strip
+  // reads written words directly, and needs the progress word only for chunks that are never
+  // written (skipped as dead: every jump publishes) and for its tag scan behind the band, so
+  // in-band flushes publish every 8th chunk and skip the fence's round trip otherwise.
+  auto flush = [&](int k, bool publish) {
+    const long long tf0 = wa.prof ? clock64() : 0;
     const int col = (k << 5) + lane;
     __syncwarp();
     const double v = out_row[((k & 1) << 5) + lane];
@@ -347,8 +353,17 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         }
         out_prog->last_live = (unsigned)k;
       }
-      __threadfence();
-      st_release(&out_prog->word, ((unsigned long long)E << 32) | (unsigned)min((k + 1) << 5, C));
+      if (publish) {
+        __threadfence();
+        st_release(&out_prog->word, ((unsigned long long)E << 32) | (unsigned)min((k + 1) << 5, C));
+      }
+    }
+    if (wa.prof) {
+      __syncwarp();
+      if (lane == 0) {
+        atomicAdd(&wa.prof[11], (unsigned long long)(clock64() - tf0));
+        atomicAdd(&wa.prof[12], 1ull);
+      }
     }
   };
   auto publish_cols = [&](int cols) {
@@ -389,7 +404,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   int c = 0;
   while (!dead_tail && (c << 5) < nsteps) {
     if (has_cons)
-      while (next_flush <= c - 2) flush(next_flush++);
+      while (next_flush <= c - 2) {
+        flush(next_flush, (next_flush & 7) == 7);
+        ++next_flush;
+      }
     double inreg = dead_value<KIND>();
     bool in_live = false;
     bool fast = false;
@@ -442,10 +460,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       // actual one overwrites it), so the next strip moves to this strip's band and starts
       // its tile about two chunks before that flush.  Any value the consumer reads is a valid
       // lower bound, so no release is needed.
-      if (has_cons && lane == 0 && first_live_out == kNone) {
-        out_prog->first_live = (unsigned)c;
-        __threadfence();
-      }
+      if (has_cons && lane == 0 && first_live_out == kNone) out_prog->first_live = (unsigned)c;
     }
     if (trace && in_live && !traced_in) {
       traced_in = true;
@@ -514,8 +529,12 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
             atomicAdd(&wa.prof[6], 1ull);
           }
         }
+        // (published below: by publish_cols at the jump, or at the end of the strip)
         if (has_cons)
-          while (next_flush <= c - 1) flush(next_flush++);
+          while (next_flush <= c - 1) {
+            flush(next_flush, false);
+            ++next_flush;
+          }
         if (nc >= 0 && pending == nc) {
           // the speculative cold-start tile is the one we need: keep it
         } else if (!drop_pending()) {
@@ -616,7 +635,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
 
   if (status == 0 && has_cons) {
     if (!dead_tail) {
-      while (next_flush < nout) flush(next_flush++);
+      while (next_flush < nout) {
+        flush(next_flush, true);
+        ++next_flush;
+      }
     } else {
       publish_cols(C);
     }
