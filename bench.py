@@ -42,7 +42,7 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
 DEC_DRAM_BYTES_20K = 2.408192e6
-COARSE_UB = 4  # the learned form's upper bound: inflated DFD of every 4th point (rfd.h coarse_ub)
+COARSE_UB = 6  # the learned form's upper bound: inflated DFD of every 6th point (rfd.h coarse_ub)
 DFD_DRAM_BYTES_200K = 1.10e9 + 1.20e9
 KERNEL_OF_PHASE = {"dfd": "dfd_kernel<8>", "vefd": "team_kernel<K_VEFD>",
                    "search": "team_kernel<K_DEC>"}

@@ -191,12 +191,17 @@ __global__ void __launch_bounds__(kBlock) wave_kernel(WaveArgs wa) {
 
 // Coarse upper bound (rfd_options.coarse_ub = k), step 1: the anchors (every k-th point
 // and the last) of both curves into the coarse pair's arrays, with an inflation as extra
-// coordinate: the largest distance from a point of either block next to the anchor to the
-// end points of its block.  A monotone coupling of the anchors extends, block by block, to
-// the full point sequences, each full pair lying within the inflations of a coupled anchor
-// pair; so the DFD of the anchors with cell weights (|a - b| + inflation(a) + inflation(b))^2
-// is at least the DFD of the curves.  One block per pair (grid-stride); pairs with
-// coarse = 0 keep the DFD.
+// coordinate.  The interior points of the block between anchors lo and hi split at the
+// middle index into a prefix, charged to lo, and a suffix, charged to hi; an anchor's
+// inflation is the larger of the radius of the suffix before it (largest distance of a
+// suffix point to the anchor) and of the prefix after it.  A monotone coupling of the anchors
+// extends block by block to the full point sequences: on a step that advances one curve, its
+// prefix points pair with the anchor that stays and its suffix points with the same anchor
+// again, now coupled to the next anchor; on a diagonal step prefixes pair with prefixes, then
+// suffixes with suffixes.  Every full pair then lies within |a - b| + inflation(a) +
+// inflation(b) of a coupled anchor pair (a, b), so the DFD of the anchors with those cell
+// weights, squared, is at least the DFD of the curves.  One block per pair (grid-stride);
+// pairs with coarse = 0 keep the DFD.
 __global__ void coarse_prep_kernel(const PairDesc* pairs, const PairDesc* coarse, PairState* st,
                                    int npairs, int k) {
   for (int p = blockIdx.x; p < npairs; p += gridDim.x) {
@@ -210,30 +215,35 @@ __global__ void coarse_prep_kernel(const PairDesc* pairs, const PairDesc* coarse
       double* Y = const_cast<double*>(side ? cd.Q : cd.P);
       const long long n = side ? pd.n2 : pd.n1, cn = side ? cd.n2 : cd.n1;
       auto anchor = [&](long long a) { return exact ? a : (a == cn - 1 ? n - 1 : a * k); };
-      // largest distance from a point of block b (anchors b, b+1) to the block's end points
-      auto block_span = [&](long long b) {
-        const long long lo = anchor(b), hi = anchor(b + 1);
+      // squared distance of point i to point j
+      auto dist2 = [&](long long i, long long j) {
         double m = 0.0;
-        for (long long i = lo; i <= hi; ++i) {
-          double d1 = 0.0, d2 = 0.0;
-          for (int e = 0; e < d; ++e) {
-            const double t1 = __dsub_rn(X[i * d + e], X[lo * d + e]);
-            const double t2 = __dsub_rn(X[i * d + e], X[hi * d + e]);
-            d1 = __fma_rn(t1, t1, d1);
-            d2 = __fma_rn(t2, t2, d2);
-          }
-          m = fmax(m, fmax(d1, d2));
+        for (int e = 0; e < d; ++e) {
+          const double t = __dsub_rn(X[i * d + e], X[j * d + e]);
+          m = __fma_rn(t, t, m);
+        }
+        return m;
+      };
+      // block b (anchors b, b+1): the radius of its prefix around its first anchor (head) or
+      // of its suffix around its last anchor (tail)
+      auto block_radius = [&](long long b, bool tail) {
+        const long long lo = anchor(b), hi = anchor(b + 1), mid = lo + (hi - lo) / 2;
+        double m = 0.0;
+        if (tail) {
+          for (long long i = mid + 1; i < hi; ++i) m = fmax(m, dist2(i, hi));
+        } else {
+          for (long long i = lo + 1; i <= mid && i < hi; ++i) m = fmax(m, dist2(i, lo));
         }
         return __dsqrt_rn(m);
       };
-      // each anchor: its coordinates and the larger span of its two blocks (each block's span
-      // is computed by both of its anchors: no thread reads another's result)
+      // each anchor: its coordinates and its inflation (each block's radii are computed by
+      // its own two anchors: no thread reads another's result)
       for (long long a = threadIdx.x; a < cn; a += blockDim.x) {
         const long long at = anchor(a);
         for (int e = 0; e < d; ++e) Y[a * ds + e] = X[at * d + e];
-        const double left = !exact && a > 0 ? block_span(a - 1) : 0.0;
-        const double right = !exact && a + 1 < cn ? block_span(a) : 0.0;
-        Y[a * ds + d] = fmax(left, right);
+        const double before = !exact && a > 0 ? block_radius(a - 1, true) : 0.0;
+        const double after = !exact && a + 1 < cn ? block_radius(a, false) : 0.0;
+        Y[a * ds + d] = fmax(before, after);
       }
     }
   }
