@@ -21,9 +21,10 @@ def walk_pair(seed, n1, n2, d=2, noise=0.05):
     return P, base + rng.normal(scale=noise, size=(n2, d))
 
 
-# sizes around the 32-row strip and 32-column chunk boundaries, both orientations
+# sizes around the 32-row strip and 32-column chunk boundaries (and multiples), both orientations
 SIZES = [(2, 2), (2, 40), (40, 2), (3, 3), (31, 31), (32, 33), (33, 32), (34, 65), (65, 34),
-         (64, 64), (97, 130), (200, 150), (257, 31), (31, 257)]
+         (64, 64), (63, 40), (66, 70), (97, 130), (129, 50), (130, 129), (200, 150), (257, 31),
+         (31, 257)]
 
 
 @pytest.mark.parametrize("n1,n2", SIZES)
