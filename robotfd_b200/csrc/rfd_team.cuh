@@ -14,6 +14,8 @@
 // solo strip's (same functions), so results are bit-identical.
 #pragma once
 
+#include <type_traits>
+
 #include "rfd_device.cuh"
 #include "rfd_filter.h"
 
@@ -578,42 +580,51 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     const double2* T0 = tiles + (size_t)slot * TileT<KIND>::vals * 1024;
     const double2* T1 = T0 + 1024;
     const long long ts0 = wa.prof ? clock64() : 0;
+    // 32 steps.  The step is issue-bound rather than latency-bound, so chunks whose every
+    // cell lies inside the grid (all rows of the strip valid, columns 0 <= j < C - 1) take a
+    // body without the activity selects and the last-cell bookkeeping; others take the full
+    // one.  Both compute the same values.
+    auto steps = [&](auto interior) {
+      constexpr bool IN = decltype(interior)::value;
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
-      // tile reads and the input broadcast do not depend on the previous step
-      const double2 ta = T0[(u << 5) + lane];
-      const double2 tb = KIND == K_DEC ? T1[(u << 5) + lane] : ta;
-      const double lin = __shfl_sync(kFull, inreg, u);
-      const double lup = __shfl_up_sync(kFull, carry, 1);
-      const double left = lane == 0 ? lin : lup;
-      const int j = (c << 5) + u - lane;
-      const bool act = rowv && j >= 0 && j < C;
-      double ncarry, nbot, nres;
-      if (KIND == K_DEC) {
-        // same propagation as the solo cell, written with selects (no divergence)
-        const double rLB = ta.x, rUB = ta.y, tLB = tb.x, tUB = tb.y;
-        const bool bdead = bot < 0.0, ldead = left < 0.0;
-        const bool rinv = (left > rUB) || ldead;
-        const bool tinv = (bot > tUB) || bdead;
-        const double rm = dmax(rLB, left);
-        const double tm = dmax(tLB, bot);
-        ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
-        nres = bdead ? (rinv ? -2.0 : rUB) : rUB;
-        nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
-      } else {
-        const double in = dmin(left, bot);
-        const double top = dmax(ta.x, in);
-        const double right = dmax(ta.y, in);
-        ncarry = right;
-        nbot = top;
-        nres = dmin(top, right);
+      for (int u = 0; u < 32; ++u) {
+        // tile reads and the input broadcast do not depend on the previous step
+        const double2 ta = T0[(u << 5) + lane];
+        const double2 tb = KIND == K_DEC ? T1[(u << 5) + lane] : ta;
+        const double lin = __shfl_sync(kFull, inreg, u);
+        const double lup = __shfl_up_sync(kFull, carry, 1);
+        const double left = lane == 0 ? lin : lup;
+        const int j = (c << 5) + u - lane;
+        const bool act = IN || (rowv && j >= 0 && j < C);
+        double ncarry, nbot, nres;
+        if (KIND == K_DEC) {
+          // same propagation as the solo cell, written with selects (no divergence)
+          const double rLB = ta.x, rUB = ta.y, tLB = tb.x, tUB = tb.y;
+          const bool bdead = bot < 0.0, ldead = left < 0.0;
+          const bool rinv = (left > rUB) || ldead;
+          const bool tinv = (bot > tUB) || bdead;
+          const double rm = dmax(rLB, left);
+          const double tm = dmax(tLB, bot);
+          ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
+          nres = IN ? 0.0 : (bdead ? (rinv ? -2.0 : rUB) : rUB);
+          nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
+        } else {
+          const double in = dmin(left, bot);
+          const double top = dmax(ta.x, in);
+          const double right = dmax(ta.y, in);
+          ncarry = right;
+          nbot = top;
+          nres = IN ? 0.0 : dmin(top, right);
+        }
+        carry = act ? ncarry : carry;
+        bot = act ? nbot : bot;
+        if (!IN && act && last_row && j == C - 1) res = nres;
+        // lane 31 produced column (c << 5) + u - 31 of the strip's last row
+        if (lane == 31) out_row[((c << 5) + u - 31) & 63] = carry;
       }
-      carry = act ? ncarry : carry;
-      bot = act ? nbot : bot;
-      if (act && last_row && j == C - 1) res = nres;
-      // lane 31 produced column (c << 5) + u - 31 of the strip's last row
-      if (lane == 31) out_row[((c << 5) + u - 31) & 63] = carry;
-    }
+    };
+    if (c >= 1 && (c << 5) + 33 <= C && (s + 1) * 32 <= R) steps(std::true_type{});
+    else steps(std::false_type{});
     if (wa.prof && lane == 0) {
       atomicAdd(&wa.prof[3], (unsigned long long)(clock64() - ts0));
       atomicAdd(&wa.prof[5], 1ull);
