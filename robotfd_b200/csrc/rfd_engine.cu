@@ -534,7 +534,7 @@ struct rfd_context {
   int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
   int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
   int dfd_grid[2] = {0, 0};  // [stacked, skewed]
-  int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 4 rows per lane
+  int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 1 row per lane
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
   size_t dws_size = 0;
@@ -917,7 +917,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       ++launches;
     }
     // the inflated (coarse) sweep always runs 4 rows per lane (its point records are wider)
-    const int rows = ck ? 4 : ctx->dfd_rows;
+    // The coarse pair has k times fewer points per curve: one row per lane gives its sweep
+    // the most strips in flight (long pair, k = 6: 21 ms against 38 with four rows).
+    const int rows = ck ? 1 : ctx->dfd_rows;
     {
       const int gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
       const int gx = std::max(32, 8 * ctx->num_sms / gy);
@@ -938,8 +940,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                                          : (strips < 2 * (int64_t)grid[1] * (kBlock / 32) ? 1 : 0);
       const int g = grid[sk];
       switch (ck ? 100 + sk : ctx->dfd_rows * 2 + sk) {
-        case 100: dfd_kernel<4, false, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 101: dfd_kernel<4, true, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 100: dfd_kernel<1, false, true><<<g, kBlock, 0, st>>>(wa); break;
+        case 101: dfd_kernel<1, true, true><<<g, kBlock, 0, st>>>(wa); break;
         case 2: dfd_kernel<1, false><<<g, kBlock, 0, st>>>(wa); break;
         case 3: dfd_kernel<1, true><<<g, kBlock, 0, st>>>(wa); break;
         case 4: dfd_kernel<2, false><<<g, kBlock, 0, st>>>(wa); break;
@@ -1172,8 +1174,8 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
       }
       c->dfd_grid[sk] = std::max(1, od) * c->num_sms;
       od = 0;
-      if (sk) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, true, true>, kBlock, 0);
-      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, false, true>, kBlock, 0);
+      if (sk) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, true, true>, kBlock, 0);
+      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, false, true>, kBlock, 0);
       c->dfd_grid_infl[sk] = std::max(1, od) * c->num_sms;
     }
     const char* pe = getenv("RFD_PROF");
