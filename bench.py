@@ -41,12 +41,14 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
             "20-knot time warp, noise 0.1, seed 1); FD to 2^-33 relative")
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
-DEC_DRAM_BYTES_20K = 2.408192e6
+DEC_DRAM_BYTES_20K = 3.730432e6   # ncu, one decision launch of the 20,000-point case
+VEFD_DRAM_BYTES_20K = 4.31e6      # ncu, one VE-FD launch of the same case (two launches averaged)
 COARSE_UB = 6  # the learned form's upper bound: inflated DFD of every 6th point (rfd.h coarse_ub)
 DFD_DRAM_BYTES_200K = 1.10e9 + 1.20e9
-KERNEL_OF_PHASE = {"dfd": "dfd_kernel<8>", "vefd": "team_kernel<K_VEFD>",
-                   "search": "team_kernel<K_DEC>"}
-FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3, "vefd": lambda d: 24 * d + 2,
+KERNEL_OF_PHASE = {"dfd": f"dfd_kernel<{'1, INFL' if COARSE_UB else '8'}>",
+                   "vefd": "team_kernel<K_VEFD>", "search": "team_kernel<K_DEC>"}
+FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3 + (4 if COARSE_UB else 0),  # + sqrt, 2 adds, square
+                  "vefd": lambda d: 24 * d + 2,
                   "search": lambda d: 12 * d + 22}
 
 
@@ -388,8 +390,10 @@ def main():
     peak = ctx.fp64_peak()
     calls = max(phases["calls"], 1)
     ph_ms = {k: phases[k + "_ms"] / calls for k in ("dfd", "vefd", "search")}
+    # the learned form's DFD phase sweeps the coarse pair: anchors every COARSE_UB-th point
+    cn1, cn2 = ((n1 - 2) // COARSE_UB + 2, (n2 - 2) // COARSE_UB + 2) if COARSE_UB else (n1, n2)
     cells = {
-        "dfd": n1 * n2,
+        "dfd": cn1 * cn2,
         "vefd": res["cells_vefd"],
         "search": res["cells_evaluated"],
     }
@@ -397,12 +401,13 @@ def main():
     flops = cells[dom] * FLOPS_PER_CELL[dom](d)
     achieved = flops / (ph_ms[dom] * 1e-3) / 1e12
     traffic = None
-    if dom == "search":
-        # ncu dram__bytes_read.sum + dram__bytes_write.sum of one decision launch on the
+    if dom in ("search", "vefd"):
+        # ncu dram__bytes_read.sum + dram__bytes_write.sum of one decision (VE-FD) launch on the
         # 20,000-point case (cold cache: every touched point record and boundary word once);
         # the touched data grows with the points, not the cells, so it scales by n1 + n2
-        traffic = DEC_DRAM_BYTES_20K * (n1 + n2) / 40000
-    elif dom == "dfd":
+        per20k = DEC_DRAM_BYTES_20K if dom == "search" else VEFD_DRAM_BYTES_20K
+        traffic = per20k * (n1 + n2) / 40000
+    elif dom == "dfd" and not COARSE_UB:
         # ncu dram__bytes_read.sum + dram__bytes_write.sum of the DFD launch on the full
         # 200,000-point pair (one pass): the boundary rows the 256-row strips hand over,
         # scaled by their count for other sizes
@@ -442,7 +447,7 @@ def main():
             "evaluated": res["cells_evaluated"] / (ph_ms["search"] * 1e-3),
             "evaluated_fraction": res["cells_evaluated"] / max(res["cells_nominal"], 1),
         },
-        "bounds_cells_per_s": {"dfd": n1 * n2 / (ph_ms["dfd"] * 1e-3),
+        "bounds_cells_per_s": {"dfd": cells["dfd"] / (ph_ms["dfd"] * 1e-3),
                                "vefd_nominal": (n1 - 1) * (n2 - 1) / (ph_ms["vefd"] * 1e-3),
                                "vefd_evaluated": res["cells_vefd"] / (ph_ms["vefd"] * 1e-3)},
         "phase_ms": ph_ms,
