@@ -21,6 +21,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "rfd.h"
@@ -722,15 +723,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   const bool use_model = mode == MODE_DISTANCE && o.model && !o.bracket;
   const size_t feat_off = use_model ? take(sizeof(float) * rfd_mlp::kInputWidth * npairs) : 0;
   const size_t y_off = use_model ? take(sizeof(float) * rfd_mlp::kOutputs * npairs) : 0;
+  // host curves: one contiguous region laid out exactly as the pinned staging area below
+  // (same sizes, same 256-byte alignment), so a single copy moves every curve
+  const size_t curves_begin = off;
+  if (!on_device)
+    for (int64_t p = 0; p < npairs; ++p) {
+      L.P[p] = take(sizeof(double) * n1s[p] * dims[p]);
+      L.Q[p] = take(sizeof(double) * n2s[p] * dims[p]);
+    }
+  const size_t curves_end = off;
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
     const int d = dims[p];
     const int64_t S = (n1 + 31) / 32;
     const int64_t cstride = align_up((size_t)n2, 32);
-    if (!on_device) {
-      L.P[p] = take(sizeof(double) * n1 * d);
-      L.Q[p] = take(sizeof(double) * n2 * d);
-    }
     L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(n1 - 1, 1));
     L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(n2 - 1, 1));
     L.bnd[p] = take(sizeof(double) * (S > 1 ? S - 1 : 0) * cstride);
@@ -780,14 +786,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     if (on_device) {
       D.P = c1s[p];
       D.Q = c2s[p];
-    } else if (drop) {
-      copy_kept((double*)(hbase + L.hP[p]), c1s[p], in_n1s[p], d);
-      copy_kept((double*)(hbase + L.hQ[p]), c2s[p], in_n2s[p], d);
-      D.P = (const double*)(dbase + L.P[p]);
-      D.Q = (const double*)(dbase + L.Q[p]);
-    } else {
-      memcpy(hbase + L.hP[p], c1s[p], sizeof(double) * n1 * d);
-      memcpy(hbase + L.hQ[p], c2s[p], sizeof(double) * n2 * d);
+    } else {  // staged below
       D.P = (const double*)(dbase + L.P[p]);
       D.Q = (const double*)(dbase + L.Q[p]);
     }
@@ -846,6 +845,47 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       }
   }
 
+  if (!on_device) {
+    // Copy every curve into the pinned staging area (compacting repeated points with
+    // drop_repeats).  Large batches split the pairs over host threads by bytes: a single
+    // thread copying pageable memory was a good part of a 4096-pair call.
+    auto work = [&](int64_t p0, int64_t p1) {
+      for (int64_t p = p0; p < p1; ++p) {
+        const int d = dims[p];
+        if (drop) {
+          copy_kept((double*)(hbase + L.hP[p]), c1s[p], in_n1s[p], d);
+          copy_kept((double*)(hbase + L.hQ[p]), c2s[p], in_n2s[p], d);
+        } else {
+          memcpy(hbase + L.hP[p], c1s[p], sizeof(double) * n1s[p] * d);
+          memcpy(hbase + L.hQ[p], c2s[p], sizeof(double) * n2s[p] * d);
+        }
+      }
+    };
+    const size_t bytes = curves_end - curves_begin;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = bytes >= ((size_t)32 << 20) ? (int)std::min(8u, std::max(1u, hw)) : 1;
+    bool done = false;
+    if (nt > 1) {
+      std::vector<int64_t> cut(nt + 1, npairs);
+      cut[0] = 0;
+      size_t acc = 0;
+      int k = 1;
+      for (int64_t p = 0; p < npairs && k < nt; ++p) {
+        acc += sizeof(double) * (size_t)(in_n1s[p] + in_n2s[p]) * dims[p];
+        if (acc >= bytes / nt * k) cut[k++] = p + 1;
+      }
+      try {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t) th.emplace_back(work, cut[t], cut[t + 1]);
+        for (auto& t : th) t.join();
+        done = true;
+      } catch (...) {
+        done = false;  // no thread could be started: copy on this one
+      }
+    }
+    if (!done) work(0, npairs);
+  }
+
   // ---------------- transfers
   cudaStream_t st = ctx->stream;
   size_t h2d_bytes = sizeof(PairDesc) * npairs + sizeof(PairState) * npairs + sizeof(int2) * nitems +
@@ -863,14 +903,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                            cudaMemcpyHostToDevice, st));
   RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
                            cudaMemcpyHostToDevice, st));
-  if (!on_device) {
-    // curves are staged contiguously; one copy per pair keeps device offsets independent
-    for (int64_t p = 0; p < npairs; ++p) {
-      RFD_CUDA(cudaMemcpyAsync(dbase + L.P[p], hbase + L.hP[p], sizeof(double) * n1s[p] * dims[p],
-                               cudaMemcpyHostToDevice, st));
-      RFD_CUDA(cudaMemcpyAsync(dbase + L.Q[p], hbase + L.hQ[p], sizeof(double) * n2s[p] * dims[p],
-                               cudaMemcpyHostToDevice, st));
-    }
+  if (!on_device && curves_end > curves_begin) {
+    // the device curve region mirrors the staging area byte for byte: one copy
+    RFD_CUDA(cudaMemcpyAsync(dbase + curves_begin, hbase + L.h_curves, curves_end - curves_begin,
+                             cudaMemcpyHostToDevice, st));
   }
   RFD_CUDA(cudaMemsetAsync(dbase + L.zero_begin, 0, L.zero_end - L.zero_begin, st));
   int* hmisc = (int*)(hbase + L.h_misc);  // [0] active pairs, [1] error word read back
