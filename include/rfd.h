@@ -78,9 +78,10 @@ typedef struct rfd_options {
   int32_t coarse_ub;        /* 0: the DFD is the upper bound (the reference's method).  k in
                                [2, 4096] (needs reference_quirks = 0): the upper bound is the DFD of
                                every k-th point and the last, each cell weighted by the distance
-                               plus both points' inflations (the largest distance of a point of an
-                               adjacent block to its block's end points): a certified bound on
-                               the DFD from k*k times fewer cells.  result.dfd then holds that
+                               plus both points' inflations (an anchor's inflation: the largest
+                               distance to it of the half-blocks it covers, the suffix of the block
+                               before it and the prefix of the block after it): a certified bound
+                               on the DFD from k*k times fewer cells.  result.dfd then holds that
                                bound (RFD_FLAG_DFD_COARSE).  The FD, within the stop rule, does
                                not depend on it. */
   int32_t drop_repeats;     /* 1: drop consecutive repeated points (all coordinates equal) from
@@ -93,6 +94,10 @@ typedef struct rfd_options {
                                reference's text loaders drop such points (include/txtReader.hpp:
                                36-41); this applies the same rule to curves built in code.
                                0 (default) keeps the reference's behaviour. */
+  int32_t graph;            /* 1: capture the call's device work (copies, launches, read-back)
+                               as one CUDA graph and keep it in the context; a later call with
+                               the same layout (pair sizes, options, workspace, stream) replays
+                               it instead of issuing each launch.  Results are identical. */
 } rfd_options;
 
 typedef struct rfd_result {

@@ -79,6 +79,7 @@ class Options(ctypes.Structure):
         ("model", ctypes.c_void_p),
         ("coarse_ub", ctypes.c_int32),
         ("drop_repeats", ctypes.c_int32),
+        ("graph", ctypes.c_int32),
     ]
 
 
@@ -216,7 +217,7 @@ def _curve(c):
 
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
-            precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False):
+            precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False, graph=False):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -231,6 +232,7 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
         o.model = model._h.value
     o.coarse_ub = int(coarse_ub)
     o.drop_repeats = int(bool(drop_repeats))
+    o.graph = int(bool(graph))
     return o
 
 

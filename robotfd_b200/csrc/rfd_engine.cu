@@ -546,6 +546,11 @@ struct rfd_context {
   int timing = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  // rfd_options.graph: the last call's work as an instantiated CUDA graph, and the layout it
+  // was captured for (a call with the same layout replays it)
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t gkey = 0;
+  int glaunches = 0;
 };
 
 namespace {
@@ -892,153 +897,217 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                      sizeof(int);
   if (!on_device)
     for (int64_t p = 0; p < npairs; ++p) h2d_bytes += sizeof(double) * (n1s[p] + n2s[p]) * dims[p];
-  RFD_CUDA(cudaMemcpyAsync(dbase + L.descs, hbase + L.h_descs, sizeof(PairDesc) * npairs,
-                           cudaMemcpyHostToDevice, st));
-  if (ck) {
-    RFD_CUDA(cudaMemcpyAsync(dbase + cdescs, hbase + h_cdescs, sizeof(PairDesc) * npairs,
-                             cudaMemcpyHostToDevice, st));
-    h2d_bytes += sizeof(PairDesc) * npairs;
-  }
-  RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * npairs,
-                           cudaMemcpyHostToDevice, st));
-  RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
-                           cudaMemcpyHostToDevice, st));
-  if (!on_device && curves_end > curves_begin) {
-    // the device curve region mirrors the staging area byte for byte: one copy
-    RFD_CUDA(cudaMemcpyAsync(dbase + curves_begin, hbase + L.h_curves, curves_end - curves_begin,
-                             cudaMemcpyHostToDevice, st));
-  }
-  RFD_CUDA(cudaMemsetAsync(dbase + L.zero_begin, 0, L.zero_end - L.zero_begin, st));
   int* hmisc = (int*)(hbase + L.h_misc);  // [0] active pairs, [1] error word read back
   hmisc[0] = (int)npairs;
   hmisc[1] = 0;
-  RFD_CUDA(cudaMemcpyAsync(dbase + L.active, hmisc, sizeof(int), cudaMemcpyHostToDevice, st));
+  const rfd_model* gmodel = use_model ? o.model : nullptr;
+  if (gmodel) {  // activation buffers allocated now: the launches below allocate nothing
+    const int rc = rfd_mlp::reserve(const_cast<rfd_model*>(gmodel), (int)npairs);
+    if (rc) return rc;
+  }
 
-  // ---------------- launches
-  const PairDesc* dd = (const PairDesc*)(dbase + L.descs);
-  PairState* ds = (PairState*)(dbase + L.states);
-  const int start_phase = mode == MODE_DECIDE ? PH_SEARCH : PH_DFD;
-  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[0], st));
-  int launches = 1;
-  prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dd, ds, (int)npairs,
-                                                                                start_phase);
-  RFD_CUDA(cudaGetLastError());
-  WaveArgs wa;
-  wa.pairs = dd;
-  wa.st = ds;
-  wa.items = (const int2*)(dbase + L.items);
-  wa.nitems = L.nitems;
-  wa.error = (int*)(dbase + L.error);
-  wa.active_pairs = (int*)(dbase + L.active);
-  wa.spin_cycles = ctx->spin_cycles;
-  wa.prof = ctx->prof ? (unsigned long long*)(dbase + prof_off) : nullptr;
-  unsigned* counters = (unsigned*)(dbase + L.counters);
-  int li = 0;
-  // boundary rows of the pairs about to run `ph` back to "not yet written" (team strips)
-  // (at least 32 blocks per pair: late probe rounds leave a few large pairs active)
-  const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
-  const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
-  auto fill = [&](int ph) {
-    bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dd, ds, (int)npairs, ph);
-    ++launches;
-  };
-  if (mode != MODE_DECIDE) {
-    wa.phase = PH_DFD;
-    wa.ticket = counters + li++;
-    // the DFD sweep runs on the coarse pairs when the coarse upper bound is asked for
-    const PairDesc* ddfd = ck ? (const PairDesc*)(dbase + cdescs) : dd;
+  // Transfers, launches and the results' read-back.  With rfd_options.graph they are captured
+  // as one CUDA graph; a later call with the same layout (sizes, options, workspace) replays it,
+  // reading the new inputs from the same pinned staging area.
+  int launches = 0;
+  auto issue = [&]() -> int {
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.descs, hbase + L.h_descs, sizeof(PairDesc) * npairs,
+                             cudaMemcpyHostToDevice, st));
     if (ck) {
-      coarse_prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(
-          dd, ddfd, ds, (int)npairs, ck);
-      ++launches;
+      RFD_CUDA(cudaMemcpyAsync(dbase + cdescs, hbase + h_cdescs, sizeof(PairDesc) * npairs,
+                               cudaMemcpyHostToDevice, st));
+      h2d_bytes += sizeof(PairDesc) * npairs;
     }
-    // the inflated (coarse) sweep always runs 4 rows per lane (its point records are wider)
-    // The coarse pair has k times fewer points per curve: one row per lane gives its sweep
-    // the most strips in flight (long pair, k = 6: 21 ms against 38 with four rows).
-    const int rows = ck ? 1 : ctx->dfd_rows;
-    {
-      const int gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
-      const int gx = std::max(32, 8 * ctx->num_sms / gy);
-      dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(ddfd, (int)npairs, 32 * rows);
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * npairs,
+                             cudaMemcpyHostToDevice, st));
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
+                             cudaMemcpyHostToDevice, st));
+    if (!on_device && curves_end > curves_begin) {
+      // the device curve region mirrors the staging area byte for byte: one copy
+      RFD_CUDA(cudaMemcpyAsync(dbase + curves_begin, hbase + L.h_curves, curves_end - curves_begin,
+                               cudaMemcpyHostToDevice, st));
     }
-    ++launches;
-    wa.pairs = ddfd;
-    {
-      // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
-      // latency decides), stacked rows otherwise (instruction throughput decides)
-      int64_t strips = 0;
-      for (int64_t p = 0; p < npairs; ++p) {
-        const int64_t n1 = ck && n1s[p] >= 2 && n2s[p] >= 2 ? coarse_n(n1s[p]) : n1s[p];
-        strips += (n1 + 32 * rows - 1) / (32 * rows);
-      }
-      const int* grid = ck ? ctx->dfd_grid_infl : ctx->dfd_grid;
-      const int sk = ctx->dfd_skew >= 0 ? ctx->dfd_skew
-                                         : (strips < 2 * (int64_t)grid[1] * (kBlock / 32) ? 1 : 0);
-      const int g = grid[sk];
-      switch (ck ? 100 + sk : ctx->dfd_rows * 2 + sk) {
-        case 100: dfd_kernel<1, false, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 101: dfd_kernel<1, true, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 2: dfd_kernel<1, false><<<g, kBlock, 0, st>>>(wa); break;
-        case 3: dfd_kernel<1, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 4: dfd_kernel<2, false><<<g, kBlock, 0, st>>>(wa); break;
-        case 5: dfd_kernel<2, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 8: dfd_kernel<4, false><<<g, kBlock, 0, st>>>(wa); break;
-        case 9: dfd_kernel<4, true><<<g, kBlock, 0, st>>>(wa); break;
-        case 16: dfd_kernel<8, false><<<g, kBlock, 0, st>>>(wa); break;
-        default: dfd_kernel<8, true><<<g, kBlock, 0, st>>>(wa); break;
-      }
-    }
-    wa.pairs = dd;
+    RFD_CUDA(cudaMemsetAsync(dbase + L.zero_begin, 0, L.zero_end - L.zero_begin, st));
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.active, hmisc, sizeof(int), cudaMemcpyHostToDevice, st));
+
+    // ---------------- launches
+    const PairDesc* dd = (const PairDesc*)(dbase + L.descs);
+    PairState* ds = (PairState*)(dbase + L.states);
+    const int start_phase = mode == MODE_DECIDE ? PH_SEARCH : PH_DFD;
+    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[0], st));
+    launches = 1;
+    prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dd, ds, (int)npairs,
+                                                                                  start_phase);
     RFD_CUDA(cudaGetLastError());
-    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
-    for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
-      wa.phase = ph;
+    WaveArgs wa;
+    wa.pairs = dd;
+    wa.st = ds;
+    wa.items = (const int2*)(dbase + L.items);
+    wa.nitems = L.nitems;
+    wa.error = (int*)(dbase + L.error);
+    wa.active_pairs = (int*)(dbase + L.active);
+    wa.spin_cycles = ctx->spin_cycles;
+    wa.prof = ctx->prof ? (unsigned long long*)(dbase + prof_off) : nullptr;
+    unsigned* counters = (unsigned*)(dbase + L.counters);
+    int li = 0;
+    // boundary rows of the pairs about to run `ph` back to "not yet written" (team strips)
+    // (at least 32 blocks per pair: late probe rounds leave a few large pairs active)
+    const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
+    const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
+    auto fill = [&](int ph) {
+      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dd, ds, (int)npairs, ph);
+      ++launches;
+    };
+    if (mode != MODE_DECIDE) {
+      wa.phase = PH_DFD;
+      wa.ticket = counters + li++;
+      // the DFD sweep runs on the coarse pairs when the coarse upper bound is asked for
+      const PairDesc* ddfd = ck ? (const PairDesc*)(dbase + cdescs) : dd;
+      if (ck) {
+        coarse_prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(
+            dd, ddfd, ds, (int)npairs, ck);
+        ++launches;
+      }
+        // The coarse pair has k times fewer points per curve: one row per lane gives its sweep
+      // the most strips in flight (long pair, k = 6: 21 ms against 38 with four rows).
+      const int rows = ck ? 1 : ctx->dfd_rows;
+      {
+        const int gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
+        const int gx = std::max(32, 8 * ctx->num_sms / gy);
+        dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(ddfd, (int)npairs, 32 * rows);
+      }
+      ++launches;
+      wa.pairs = ddfd;
+      {
+        // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
+        // latency decides), stacked rows otherwise (instruction throughput decides)
+        int64_t strips = 0;
+        for (int64_t p = 0; p < npairs; ++p) {
+          const int64_t n1 = ck && n1s[p] >= 2 && n2s[p] >= 2 ? coarse_n(n1s[p]) : n1s[p];
+          strips += (n1 + 32 * rows - 1) / (32 * rows);
+        }
+        const int* grid = ck ? ctx->dfd_grid_infl : ctx->dfd_grid;
+        const int sk = ctx->dfd_skew >= 0 ? ctx->dfd_skew
+                                           : (strips < 2 * (int64_t)grid[1] * (kBlock / 32) ? 1 : 0);
+        const int g = grid[sk];
+        switch (ck ? 100 + sk : ctx->dfd_rows * 2 + sk) {
+          case 100: dfd_kernel<1, false, true><<<g, kBlock, 0, st>>>(wa); break;
+          case 101: dfd_kernel<1, true, true><<<g, kBlock, 0, st>>>(wa); break;
+          case 2: dfd_kernel<1, false><<<g, kBlock, 0, st>>>(wa); break;
+          case 3: dfd_kernel<1, true><<<g, kBlock, 0, st>>>(wa); break;
+          case 4: dfd_kernel<2, false><<<g, kBlock, 0, st>>>(wa); break;
+          case 5: dfd_kernel<2, true><<<g, kBlock, 0, st>>>(wa); break;
+          case 8: dfd_kernel<4, false><<<g, kBlock, 0, st>>>(wa); break;
+          case 9: dfd_kernel<4, true><<<g, kBlock, 0, st>>>(wa); break;
+          case 16: dfd_kernel<8, false><<<g, kBlock, 0, st>>>(wa); break;
+          default: dfd_kernel<8, true><<<g, kBlock, 0, st>>>(wa); break;
+        }
+      }
+      wa.pairs = dd;
+      RFD_CUDA(cudaGetLastError());
+      if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
+      for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
+        wa.phase = ph;
+        wa.ticket = counters + li++;
+        if (ctx->solo) {
+          wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
+        } else {
+          fill(ph);
+          team_kernel<K_VEFD><<<ctx->team_grid[K_VEFD], kTeamThreads, team_smem_bytes<K_VEFD>(), st>>>(wa);
+        }
+        RFD_CUDA(cudaGetLastError());
+      }
+      launches += 3;
+      if (use_model) {
+        rfd_model* md = const_cast<rfd_model*>(o.model);
+        if (rfd_mlp::model_device(md) != ctx->device)
+          return fail(RFD_ERR_ARG, "the model lives on another device");
+        float* feat = (float*)(dbase + feat_off);
+        float* yout = (float*)(dbase + y_off);
+        bracket_features_kernel<<<(int)std::min<int64_t>(npairs, 16 * ctx->num_sms), kFeatThreads, 0,
+                                  st>>>(dd, ds, (int)npairs, feat);
+        RFD_CUDA(cudaGetLastError());
+        int rc2 = rfd_mlp::infer(md, feat, (int)npairs, yout, st);
+        if (rc2) return rc2;
+        bracket_apply_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
+            ds, (int)npairs, yout, wa.active_pairs);
+        RFD_CUDA(cudaGetLastError());
+        launches += 2 + 4;
+      }
+    }
+    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
+    const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
+    for (int k = 0; k < nprobe; ++k) {
+      wa.phase = PH_SEARCH;
       wa.ticket = counters + li++;
       if (ctx->solo) {
-        wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
+        wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
       } else {
-        fill(ph);
-        team_kernel<K_VEFD><<<ctx->team_grid[K_VEFD], kTeamThreads, team_smem_bytes<K_VEFD>(), st>>>(wa);
+        fill(PH_SEARCH);
+        team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
       }
       RFD_CUDA(cudaGetLastError());
+      ++launches;
     }
-    launches += 3;
-    if (use_model) {
-      rfd_model* md = const_cast<rfd_model*>(o.model);
-      if (rfd_mlp::model_device(md) != ctx->device)
-        return fail(RFD_ERR_ARG, "the model lives on another device");
-      float* feat = (float*)(dbase + feat_off);
-      float* yout = (float*)(dbase + y_off);
-      bracket_features_kernel<<<(int)std::min<int64_t>(npairs, 16 * ctx->num_sms), kFeatThreads, 0,
-                                st>>>(dd, ds, (int)npairs, feat);
-      RFD_CUDA(cudaGetLastError());
-      int rc2 = rfd_mlp::infer(md, feat, (int)npairs, yout, st);
-      if (rc2) return rc2;
-      bracket_apply_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
-          ds, (int)npairs, yout, wa.active_pairs);
-      RFD_CUDA(cudaGetLastError());
-      launches += 2 + 4;
-    }
-  }
-  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
-  const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
-  for (int k = 0; k < nprobe; ++k) {
-    wa.phase = PH_SEARCH;
-    wa.ticket = counters + li++;
-    if (ctx->solo) {
-      wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
-    } else {
-      fill(PH_SEARCH);
-      team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
-    }
-    RFD_CUDA(cudaGetLastError());
-    ++launches;
-  }
-  if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[3], st));
+    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[3], st));
 
-  // ---------------- results
-  RFD_CUDA(cudaMemcpyAsync(hs, ds, sizeof(PairState) * npairs, cudaMemcpyDeviceToHost, st));
-  RFD_CUDA(cudaMemcpyAsync(hmisc + 1, wa.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // ---------------- results
+    RFD_CUDA(cudaMemcpyAsync(hs, ds, sizeof(PairState) * npairs, cudaMemcpyDeviceToHost, st));
+    RFD_CUDA(cudaMemcpyAsync(hmisc + 1, wa.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return RFD_OK;
+  };
+  const bool use_graph = o.graph != 0;
+  uint64_t key = 1469598103934665603ull;  // FNV-1a over everything the launches depend on
+  auto mix = [&](const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) key = (key ^ b[i]) * 1099511628211ull;
+  };
+  if (use_graph) {
+    const int flags[] = {mode, (int)on_device, ck, max_probes, o.stop_mode, o.reference_quirks,
+                         o.dense, o.precision, o.bracket != nullptr, ctx->timing, ctx->prof,
+                         ctx->solo, ctx->dfd_rows, ctx->dfd_skew};
+    const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
+                          (const void*)st};
+    mix(flags, sizeof(flags));
+    mix(ptrs, sizeof(ptrs));
+    mix(&o.tol, sizeof(o.tol));
+    mix(&npairs, sizeof(npairs));
+    mix(n1s, sizeof(int64_t) * npairs);
+    mix(n2s, sizeof(int64_t) * npairs);
+    mix(dims, sizeof(int32_t) * npairs);
+  }
+  if (use_graph && ctx->gexec && ctx->gkey == key) {
+    RFD_CUDA(cudaGraphLaunch(ctx->gexec, st));
+    launches = ctx->glaunches;
+  } else {
+    if (use_graph) {
+      if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+      ctx->gexec = nullptr;
+      RFD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    }
+    const int rc = issue();
+    if (use_graph) {
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(st, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ec != cudaSuccess) return fail(RFD_ERR_CUDA, std::string("cudaStreamEndCapture: ") +
+                                                          cudaGetErrorString(ec));
+      cudaGraphExec_t ex = nullptr;
+      const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) return fail(RFD_ERR_CUDA, std::string("cudaGraphInstantiate: ") +
+                                                          cudaGetErrorString(ei));
+      ctx->gexec = ex;
+      ctx->gkey = key;
+      ctx->glaunches = launches;
+      RFD_CUDA(cudaGraphLaunch(ex, st));
+    } else if (rc) {
+      return rc;
+    }
+  }
   RFD_CUDA(cudaStreamSynchronize(st));
   if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
   if (ctx->prof) {
@@ -1235,6 +1304,7 @@ int32_t rfd_context_destroy(rfd_context* ctx) {
   if (ctx->hws) cudaFreeHost(ctx->hws);
   for (int k = 0; k < 4; ++k)
     if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return RFD_OK;

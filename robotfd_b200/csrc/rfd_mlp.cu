@@ -342,6 +342,9 @@ int backward(rfd_model* md, const float* X, const float* T, int B, cudaStream_t 
 namespace rfd_mlp {
 int model_device(const rfd_model* md) { return md->device; }
 // Inference for the solver: X FP32 [B][400] (device) -> Y FP32 [B][2] (device, ld 2).
+int reserve(rfd_model* md, int B) { return ensure_cap(md, B); }
+const void* buffers_id(const rfd_model* md) { return md->Y; }
+
 int infer(rfd_model* md, const float* X, int B, float* Yout, cudaStream_t s) {
   int rc = forward(md, X, B, s);
   if (rc) return rc;

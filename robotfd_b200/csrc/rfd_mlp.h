@@ -17,6 +17,10 @@ constexpr long long kNumParams = 400LL * 256 + 256 + 256LL * 256 + 256 + 256LL *
 constexpr double kYFloor = 1e-13;
 
 int infer(rfd_model* md, const float* X, int B, float* Yout, cudaStream_t s);
+// Activation buffers for B rows, allocated ahead of a stream capture (infer then allocates
+// nothing); and an identity of those buffers (changes when they are reallocated).
+int reserve(rfd_model* md, int B);
+const void* buffers_id(const rfd_model* md);
 int model_device(const rfd_model* md);
 // records the message returned by rfd_last_error and returns code
 int set_error(int code, const char* msg);
