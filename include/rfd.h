@@ -160,6 +160,16 @@ int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const
                            const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
                            const int32_t* dims, const rfd_options* opt, rfd_result* out);
 
+/* Autotuner of the DFD sweep (no reference counterpart: the reference fixes its launch shape,
+   src/intersection_algorithm_in_parallel.cu:1268-1326).  Times rows per lane (1, 2, 4, 8: the
+   strip height) and the row layout (0 stacked, 1 skewed) on the caller's pairs, `reps` timed
+   sweeps each after one untimed one, and keeps the fastest in the context for later calls.
+   ms_out (optional): 8 doubles, ms per sweep at [rows index * 2 + layout].  best_out
+   (optional): 2 ints, the rows and layout kept.  Curves as rfd_distance_batch (opt->memory). */
+int32_t rfd_autotune(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
+                     const double* const* c2s, const int64_t* n2s, const int32_t* dims,
+                     const rfd_options* opt, int32_t reps, double* ms_out, int32_t* best_out);
+
 /* All pairwise distances of ncurves curves (no reference counterpart: the many-to-many use of
    the reference's Curves, include/curve.hpp:42-47).  out is ncurves x ncurves, row-major,
    symmetric with a zero diagonal; entry (i, j), i < j, is the distance with curve i as the

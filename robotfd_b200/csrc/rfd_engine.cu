@@ -534,7 +534,8 @@ struct rfd_context {
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
   int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
   int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
-  int dfd_grid[2] = {0, 0};  // [stacked, skewed]
+  int dfd_grid[2] = {0, 0};  // [stacked, skewed] for dfd_rows
+  int dfd_grid_all[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // for rows 1, 2, 4, 8
   int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 1 row per lane
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
   void* dws = nullptr;
@@ -1265,20 +1266,24 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
       c->dfd_rows = dr[0] - '0';
     const char* dk = getenv("RFD_DFD_SKEW");
     if (dk && (dk[0] == '0' || dk[0] == '1') && !dk[1]) c->dfd_skew = dk[0] - '0';
-    for (int sk = 0; sk < 2; ++sk) {
-      int od = 0;
-      switch (c->dfd_rows * 2 + sk) {
-        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, false>, kBlock, 0); break;
-        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, true>, kBlock, 0); break;
-        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, false>, kBlock, 0); break;
-        case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, true>, kBlock, 0); break;
-        case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, false>, kBlock, 0); break;
-        case 9: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, true>, kBlock, 0); break;
-        case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, false>, kBlock, 0); break;
-        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, true>, kBlock, 0); break;
+    for (int ri = 0; ri < 4; ++ri)
+      for (int sk = 0; sk < 2; ++sk) {
+        int od = 0;
+        switch ((1 << ri) * 2 + sk) {
+          case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, false>, kBlock, 0); break;
+          case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, true>, kBlock, 0); break;
+          case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, false>, kBlock, 0); break;
+          case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<2, true>, kBlock, 0); break;
+          case 8: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, false>, kBlock, 0); break;
+          case 9: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<4, true>, kBlock, 0); break;
+          case 16: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, false>, kBlock, 0); break;
+          default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<8, true>, kBlock, 0); break;
+        }
+        c->dfd_grid_all[ri][sk] = std::max(1, od) * c->num_sms;
       }
-      c->dfd_grid[sk] = std::max(1, od) * c->num_sms;
-      od = 0;
+    for (int sk = 0; sk < 2; ++sk) {
+      c->dfd_grid[sk] = c->dfd_grid_all[c->dfd_rows == 1 ? 0 : c->dfd_rows == 2 ? 1 : c->dfd_rows == 4 ? 2 : 3][sk];
+      int od = 0;
       if (sk) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, true, true>, kBlock, 0);
       else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&od, dfd_kernel<1, false, true>, kBlock, 0);
       c->dfd_grid_infl[sk] = std::max(1, od) * c->num_sms;
@@ -1376,6 +1381,65 @@ int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const
   if (!ctx) return fail(RFD_ERR_ARG, "null context");
   RFD_CUDA(cudaSetDevice(ctx->device));
   return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+}
+
+// Autotuner of the DFD sweep's tile shape: rows per lane (the strip height, 32 x 1, 2, 4 or 8)
+// and the layout of a lane's rows (stacked: fewer instructions per cell; skewed: independent
+// cells per step).  Each candidate sweeps the caller's pairs `reps` times (CUDA-event phase
+// times of rfd_bounds-style calls); the fastest is kept in the context for later calls, which
+// otherwise use 8 rows and choose the layout by strip count.
+int32_t rfd_autotune(rfd_context* ctx, int64_t npairs, const double* const* c1s, const int64_t* n1s,
+                     const double* const* c2s, const int64_t* n2s, const int32_t* dims,
+                     const rfd_options* opt, int32_t reps, double* ms_out, int32_t* best_out) {
+  if (!ctx || npairs < 1 || reps < 1 || reps > 100) return fail(RFD_ERR_ARG, "autotune arguments");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->ev[0])
+    for (int k = 0; k < 4; ++k) RFD_CUDA(cudaEventCreate(&ctx->ev[k]));
+  rfd_options o;
+  rfd_options_init(&o, 1);
+  if (opt) o = *opt;
+  o.graph = 0;
+  const int rows[4] = {1, 2, 4, 8};
+  const int keep_rows = ctx->dfd_rows, keep_skew = ctx->dfd_skew, keep_timing = ctx->timing;
+  double keep_acc[7];
+  memcpy(keep_acc, ctx->acc, sizeof(keep_acc));
+  std::vector<rfd_result> res((size_t)npairs);
+  double best = 1e300;
+  int best_r = keep_rows, best_s = keep_skew;
+  int rc = RFD_OK;
+  for (int ri = 0; ri < 4 && rc == RFD_OK; ++ri)
+    for (int sk = 0; sk < 2 && rc == RFD_OK; ++sk) {
+      ctx->dfd_rows = rows[ri];
+      ctx->dfd_skew = sk;
+      ctx->dfd_grid[0] = ctx->dfd_grid_all[ri][0];
+      ctx->dfd_grid[1] = ctx->dfd_grid_all[ri][1];
+      ctx->timing = 1;
+      for (int k = 0; k < 7; ++k) ctx->acc[k] = 0;
+      // one untimed call (first use of the code path), then the timed ones
+      rc = run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, &o, res.data(), MODE_BOUNDS, 0.0);
+      for (int k = 0; k < 7; ++k) ctx->acc[k] = 0;
+      for (int r = 0; r < reps && rc == RFD_OK; ++r)
+        rc = run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, &o, res.data(), MODE_BOUNDS, 0.0);
+      const double ms = rc == RFD_OK ? ctx->acc[0] / reps : -1.0;
+      if (ms_out) ms_out[ri * 2 + sk] = ms;
+      if (rc == RFD_OK && ms < best) {
+        best = ms;
+        best_r = rows[ri];
+        best_s = sk;
+      }
+    }
+  ctx->dfd_rows = rc == RFD_OK ? best_r : keep_rows;
+  ctx->dfd_skew = rc == RFD_OK ? best_s : keep_skew;
+  const int bi = ctx->dfd_rows == 1 ? 0 : ctx->dfd_rows == 2 ? 1 : ctx->dfd_rows == 4 ? 2 : 3;
+  ctx->dfd_grid[0] = ctx->dfd_grid_all[bi][0];
+  ctx->dfd_grid[1] = ctx->dfd_grid_all[bi][1];
+  ctx->timing = keep_timing;
+  memcpy(ctx->acc, keep_acc, sizeof(keep_acc));
+  if (best_out) {
+    best_out[0] = ctx->dfd_rows;
+    best_out[1] = ctx->dfd_skew;
+  }
+  return rc;
 }
 
 int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* const* curves,
