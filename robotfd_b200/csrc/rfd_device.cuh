@@ -59,7 +59,11 @@ struct PairDesc {
   double* bnd;            // [S-1][cstride] boundary rows
   unsigned int* tags;     // [S-1][tstride] epoch tag of every live chunk
   Prog* prog;             // [S]
-  int n1, n2, d, pad;
+  // tr: the team strips of a pair whose first curve is the longer run on the transposed
+  // grid (rows = curve 2), whose free intervals are the same values (the interval of an edge
+  // is the same function of its point and segment in either orientation) with the roles of
+  // the right and top edges exchanged
+  int n1, n2, d, tr;
   long long cstride, tstride;
 };
 
@@ -273,7 +277,7 @@ __device__ __forceinline__ void load_col(const PairDesc& pd, int j, ColRec<KIND,
 template <int KIND, int D>
 __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<KIND, D>& col, int i,
                                      int j, double left, double& bot, double& carry, double r2,
-                                     double& res, bool last) {
+                                     double& res, bool last, bool tr = false) {
   if (KIND == K_DFD) {
     const double dist = dist_sq<D>(row.a, col.qa);
     if (i == 0) {
@@ -323,7 +327,7 @@ __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<K
       }
       bot = tLB;
       carry = rLB;
-      if (last) res = rUB;
+      if (last) res = tr ? tUB : rUB;  // transposed grid: the right edge is the top one
     }
   }
 }
@@ -572,7 +576,8 @@ __device__ StripOut run_strip(const WaveArgs& wa, const PairDesc& pd, PairState*
       if (!dense) need = act && !(is_dead<KIND>(left, U) && is_dead<KIND>(bot, U));
       if (__any_sync(kFull, need)) {
         if (act) {
-          cell<KIND, D>(row, cur, i, j, left, bot, carry, r2, res, last_row && j == C - 1);
+          cell<KIND, D>(row, cur, i, j, left, bot, carry, r2, res, last_row && j == C - 1,
+                        pd.tr != 0);
           ++evaluated;
         }
       } else if (act) {

@@ -596,12 +596,13 @@ enum Mode { MODE_DISTANCE = 0, MODE_BOUNDS = 1, MODE_DECIDE = 2 };
 
 struct Layout {
   // device offsets
-  size_t descs, states, items, counters, error, active, zero_begin, zero_end, total;
+  size_t descs, tdescs, states, items, titems, counters, error, active, zero_begin, zero_end,
+      total;
   std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog;
   // host staging offsets
-  size_t h_descs, h_states, h_items, h_misc, h_curves, h_total;
+  size_t h_descs, h_tdescs, h_states, h_items, h_titems, h_misc, h_curves, h_total;
   std::vector<size_t> hP, hQ;
-  int nitems, nlaunch;
+  int nitems, ntitems, nlaunch;
 };
 
 int check_pair(const double* c1, int64_t n1, const double* c2, int64_t n2, int32_t d) {
@@ -695,6 +696,16 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   auto take = [&](size_t bytes) { size_t r = off; off = align_up(off + bytes, 256); return r; };
   L.descs = take(sizeof(PairDesc) * npairs);
   const size_t cdescs = ck ? take(sizeof(PairDesc) * npairs) : 0;
+  // VE-FD and decision strips run on the transposed grid when the first curve is the longer:
+  // a strip costs its 32 rows' hand-over (~7 us on B200) and a 32-column chunk ~1.8 us, so
+  // rows along the shorter curve shorten the chain of strips (50000 x 1039 points: 1563
+  // strips, 11 ms a decision, against 33).  The DFD sweeps keep the given orientation.
+  std::vector<unsigned char> trv(npairs, 0);
+  for (int64_t p = 0; p < npairs; ++p)
+    trv[p] = n1s[p] >= 2 && n2s[p] >= 2 && n1s[p] > n2s[p];
+  auto trows = [&](int64_t p) { return trv[p] ? n2s[p] : n1s[p]; };
+  auto tcols = [&](int64_t p) { return trv[p] ? n1s[p] : n2s[p]; };
+  L.tdescs = take(sizeof(PairDesc) * npairs);
   L.states = take(sizeof(PairState) * npairs);
   // items: interleave pairs by strip index so early strips of every pair go first
   std::vector<int> order(npairs);
@@ -702,25 +713,28 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     return (double)n1s[a] * (double)n2s[a] > (double)n1s[b] * (double)n2s[b];
   });
-  int64_t maxS = 0, nitems = 0;
+  int64_t maxS = 0, nitems = 0, maxSt = 0, ntitems = 0;
   for (int64_t p = 0; p < npairs; ++p) {
     int64_t S = (n1s[p] + 31) / 32;
     maxS = std::max(maxS, S);
     nitems += S;
+    const int64_t St = (trows(p) + 31) / 32;
+    maxSt = std::max(maxSt, St);
+    ntitems += St;
   }
   if (nitems > INT32_MAX / 2) return fail(RFD_ERR_LIMIT, "too many strips");
   L.nitems = (int)nitems;
+  L.ntitems = (int)ntitems;
   L.items = take(sizeof(int2) * nitems);
+  L.titems = take(sizeof(int2) * ntitems);
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0);
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * L.nlaunch);
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
   L.error = take(sizeof(int));
-  for (int64_t p = 0; p < npairs; ++p) {
-    const int64_t n1 = n1s[p], n2 = n2s[p];
-    const int64_t S = (n1 + 31) / 32;
-    const int64_t cstride = align_up((size_t)n2, 32);
-    const int64_t tstride = align_up((size_t)((n2 + 31) / 32), 32);
+  for (int64_t p = 0; p < npairs; ++p) {  // progress words and tags: team strips only
+    const int64_t S = (trows(p) + 31) / 32;
+    const int64_t tstride = align_up((size_t)((tcols(p) + 31) / 32), 32);
     L.tags[p] = take(sizeof(unsigned) * (S > 1 ? S - 1 : 0) * tstride);
     L.prog[p] = take(sizeof(Prog) * S);
   }
@@ -743,9 +757,14 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int d = dims[p];
     const int64_t S = (n1 + 31) / 32;
     const int64_t cstride = align_up((size_t)n2, 32);
-    L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(n1 - 1, 1));
-    L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(n2 - 1, 1));
-    L.bnd[p] = take(sizeof(double) * (S > 1 ? S - 1 : 0) * cstride);
+    // segment records in the team strips' orientation; boundary rows for the DFD sweep
+    // (given orientation) and the team strips
+    const int64_t St = (trows(p) + 31) / 32;
+    const int64_t tcstride = align_up((size_t)tcols(p), 32);
+    L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(trows(p) - 1, 1));
+    L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(tcols(p) - 1, 1));
+    L.bnd[p] = take(sizeof(double) * std::max((S > 1 ? S - 1 : 0) * cstride,
+                                              (St > 1 ? St - 1 : 0) * tcstride));
     if (ck) {
       // anchors and their inflations; a pair with a one-point curve keeps every point, with
       // inflation 0 (its DFD is its exact, closed-form answer)
@@ -760,8 +779,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   auto htake = [&](size_t bytes) { size_t r = hoff; hoff = align_up(hoff + bytes, 256); return r; };
   L.h_descs = htake(sizeof(PairDesc) * npairs);
   const size_t h_cdescs = ck ? htake(sizeof(PairDesc) * npairs) : 0;
+  L.h_tdescs = htake(sizeof(PairDesc) * npairs);
   L.h_states = htake(sizeof(PairState) * npairs);
   L.h_items = htake(sizeof(int2) * nitems);
+  L.h_titems = htake(sizeof(int2) * ntitems);
   L.h_misc = htake(4 * sizeof(int));
   L.h_curves = hoff;
   if (!on_device) {
@@ -807,6 +828,17 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     D.cstride = (long long)align_up((size_t)n2, 32);
     D.tstride = (long long)align_up((size_t)((n2 + 31) / 32), 32);
     (void)S;
+    PairDesc& Dt = ((PairDesc*)(hbase + L.h_tdescs))[p];
+    Dt = D;
+    if (trv[p]) {
+      Dt.P = D.Q;
+      Dt.Q = D.P;
+      Dt.n1 = (int)n2;
+      Dt.n2 = (int)n1;
+      Dt.tr = 1;
+      Dt.cstride = (long long)align_up((size_t)n1, 32);
+      Dt.tstride = (long long)align_up((size_t)((n1 + 31) / 32), 32);
+    }
     if (ck) {
       // the coarse pair: anchors of both curves, handing rows over through the pair's own
       // boundary rows (fewer rows of fewer columns).  A one-point curve keeps the exact DFD,
@@ -848,6 +880,13 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       for (int64_t q = 0; q < npairs; ++q) {
         const int p = order[q];
         if (sidx < (n1s[p] + 31) / 32) hi[k++] = make_int2(p, (int)sidx);
+      }
+    int2* ht = (int2*)(hbase + L.h_titems);
+    k = 0;
+    for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+      for (int64_t q = 0; q < npairs; ++q) {
+        const int p = order[q];
+        if (sidx < (trows(p) + 31) / 32) ht[k++] = make_int2(p, (int)sidx);
       }
   }
 
@@ -894,8 +933,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
 
   // ---------------- transfers
   cudaStream_t st = ctx->stream;
-  size_t h2d_bytes = sizeof(PairDesc) * npairs + sizeof(PairState) * npairs + sizeof(int2) * nitems +
-                     sizeof(int);
+  size_t h2d_bytes = 2 * sizeof(PairDesc) * npairs + sizeof(PairState) * npairs +
+                     sizeof(int2) * (nitems + ntitems) + sizeof(int);
   if (!on_device)
     for (int64_t p = 0; p < npairs; ++p) h2d_bytes += sizeof(double) * (n1s[p] + n2s[p]) * dims[p];
   int* hmisc = (int*)(hbase + L.h_misc);  // [0] active pairs, [1] error word read back
@@ -923,6 +962,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                              cudaMemcpyHostToDevice, st));
     RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
                              cudaMemcpyHostToDevice, st));
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.tdescs, hbase + L.h_tdescs, sizeof(PairDesc) * npairs,
+                             cudaMemcpyHostToDevice, st));
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.titems, hbase + L.h_titems, sizeof(int2) * ntitems,
+                             cudaMemcpyHostToDevice, st));
     if (!on_device && curves_end > curves_begin) {
       // the device curve region mirrors the staging area byte for byte: one copy
       RFD_CUDA(cudaMemcpyAsync(dbase + curves_begin, hbase + L.h_curves, curves_end - curves_begin,
@@ -933,18 +976,19 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
 
     // ---------------- launches
     const PairDesc* dd = (const PairDesc*)(dbase + L.descs);
+    const PairDesc* dt = (const PairDesc*)(dbase + L.tdescs);  // team strips' orientation
     PairState* ds = (PairState*)(dbase + L.states);
     const int start_phase = mode == MODE_DECIDE ? PH_SEARCH : PH_DFD;
     if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[0], st));
     launches = 1;
-    prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dd, ds, (int)npairs,
+    prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dt, ds, (int)npairs,
                                                                                   start_phase);
     RFD_CUDA(cudaGetLastError());
     WaveArgs wa;
-    wa.pairs = dd;
+    wa.pairs = dt;
     wa.st = ds;
-    wa.items = (const int2*)(dbase + L.items);
-    wa.nitems = L.nitems;
+    wa.items = (const int2*)(dbase + L.titems);
+    wa.nitems = L.ntitems;
     wa.error = (int*)(dbase + L.error);
     wa.active_pairs = (int*)(dbase + L.active);
     wa.spin_cycles = ctx->spin_cycles;
@@ -956,7 +1000,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
     const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
     auto fill = [&](int ph) {
-      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dd, ds, (int)npairs, ph);
+      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dt, ds, (int)npairs, ph);
       ++launches;
     };
     if (mode != MODE_DECIDE) {
@@ -969,7 +1013,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
             dd, ddfd, ds, (int)npairs, ck);
         ++launches;
       }
-        // The coarse pair has k times fewer points per curve: one row per lane gives its sweep
+      // The coarse pair has k times fewer points per curve: one row per lane gives its sweep
       // the most strips in flight (long pair, k = 6: 21 ms against 38 with four rows).
       const int rows = ck ? 1 : ctx->dfd_rows;
       {
@@ -978,7 +1022,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         dfd_fill_kernel<<<dim3(gx, gy), 256, 0, st>>>(ddfd, (int)npairs, 32 * rows);
       }
       ++launches;
-      wa.pairs = ddfd;
+      wa.pairs = ddfd;  // the DFD sweep: given orientation, its own item list
+      wa.items = (const int2*)(dbase + L.items);
+      wa.nitems = L.nitems;
       {
         // skewed rows when the strips cannot fill the resident warps twice over (the sweep's
         // latency decides), stacked rows otherwise (instruction throughput decides)
@@ -1004,7 +1050,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
           default: dfd_kernel<8, true><<<g, kBlock, 0, st>>>(wa); break;
         }
       }
-      wa.pairs = dd;
+      wa.pairs = dt;
+      wa.items = (const int2*)(dbase + L.titems);
+      wa.nitems = L.ntitems;
       RFD_CUDA(cudaGetLastError());
       if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
       for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {

@@ -262,6 +262,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   const bool dense = st->dense != 0;
   const bool has_prod = s > 0;
   const bool has_cons = s + 1 < S;
+  const bool tr = pd.tr != 0;
 
   Prog* in_prog = has_prod ? pd.prog + (s - 1) : nullptr;
   Prog* out_prog = has_cons ? pd.prog + s : nullptr;
@@ -606,7 +607,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
           const double rm = dmax(rLB, left);
           const double tm = dmax(tLB, bot);
           ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
-          nres = IN ? 0.0 : (bdead ? (rinv ? -2.0 : rUB) : rUB);
+          // the result is the last cell's right edge: on a transposed grid, its top edge
+          nres = IN ? 0.0
+                    : (tr ? (ldead ? (tinv ? -2.0 : tUB) : tUB)
+                          : (bdead ? (rinv ? -2.0 : rUB) : rUB));
           nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
         } else {
           const double in = dmin(left, bot);

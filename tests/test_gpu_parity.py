@@ -55,6 +55,31 @@ def test_decisions_bitexact(ctx, n1, n2, d):
             assert ub == want_ub and reach == want_reach, (e, dense, ub, want_ub)
 
 
+@pytest.mark.parametrize("n1,n2", [(70, 20), (257, 31), (40, 2), (33, 32), (20, 70)])
+@pytest.mark.parametrize("d", [2, 3])
+def test_decisions_at_the_last_corner(ctx, n1, n2, d):
+    """Pairs with a longer first curve run their decision strips on the transposed grid, whose
+    result is the last cell's top edge there.  At radii within a few ulps of the end-point
+    distance the last cell's corner sits on the ball's boundary, where the right and top
+    edges' intervals are computed from different quadratics; reach and the right edge's UB
+    must still be the oracle's, in the given orientation and in the swapped one."""
+    for seed in range(3):
+        P, Q = walk_pair(seed * 101 + n1 + n2 + d, n1, n2, d)
+        Q[0] = P[0]
+        Q[-1] = P[-1] + 3.0 / np.sqrt(d)  # the end distance is the endpoint bound
+        e = oracle.endpoint(P, Q)
+        radii = [e]
+        lo = hi = e
+        for _ in range(3):
+            lo, hi = np.nextafter(lo, 0.0), np.nextafter(hi, np.inf)
+            radii += [lo, hi]
+        for A, B in ((P, Q), (Q, P)):
+            for r in radii:
+                want = oracle.decide(A, B, r)
+                got = ctx.decide(A, B, r)
+                assert got == want, (seed, r, got, want)
+
+
 @pytest.mark.parametrize("seed,n1,n2,d", [(0, 120, 90, 2), (1, 90, 160, 3), (2, 300, 280, 2),
                                           (3, 64, 400, 3), (4, 700, 650, 3)])
 @pytest.mark.parametrize("precise", [False, True])
