@@ -950,6 +950,12 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // as one CUDA graph; a later call with the same layout (sizes, options, workspace) replays it,
   // reading the new inputs from the same pinned staging area.
   int launches = 0;
+  // Phase events.  Inside a stream capture a plain record only orders the capture; an
+  // external record becomes a graph node, so the replayed graph records the events.
+  auto record = [&](int k) {
+    return cudaEventRecordWithFlags(ctx->ev[k], st,
+                                    o.graph ? cudaEventRecordExternal : cudaEventRecordDefault);
+  };
   auto issue = [&]() -> int {
     RFD_CUDA(cudaMemcpyAsync(dbase + L.descs, hbase + L.h_descs, sizeof(PairDesc) * npairs,
                              cudaMemcpyHostToDevice, st));
@@ -979,7 +985,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const PairDesc* dt = (const PairDesc*)(dbase + L.tdescs);  // team strips' orientation
     PairState* ds = (PairState*)(dbase + L.states);
     const int start_phase = mode == MODE_DECIDE ? PH_SEARCH : PH_DFD;
-    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[0], st));
+    if (ctx->timing) RFD_CUDA(record(0));
     launches = 1;
     prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dt, ds, (int)npairs,
                                                                                   start_phase);
@@ -1054,7 +1060,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       wa.items = (const int2*)(dbase + L.titems);
       wa.nitems = L.ntitems;
       RFD_CUDA(cudaGetLastError());
-      if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[1], st));
+      if (ctx->timing) RFD_CUDA(record(1));
       for (int ph : {PH_VEFD, PH_VEFD_DENSE}) {
         wa.phase = ph;
         wa.ticket = counters + li++;
@@ -1084,7 +1090,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         launches += 2 + 4;
       }
     }
-    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[2], st));
+    if (ctx->timing) RFD_CUDA(record(2));
     const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
     for (int k = 0; k < nprobe; ++k) {
       wa.phase = PH_SEARCH;
@@ -1098,7 +1104,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       RFD_CUDA(cudaGetLastError());
       ++launches;
     }
-    if (ctx->timing) RFD_CUDA(cudaEventRecord(ctx->ev[3], st));
+    if (ctx->timing) RFD_CUDA(record(3));
 
     // ---------------- results
     RFD_CUDA(cudaMemcpyAsync(hs, ds, sizeof(PairState) * npairs, cudaMemcpyDeviceToHost, st));

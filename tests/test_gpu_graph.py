@@ -52,3 +52,21 @@ def test_graph_new_layout_and_single_pairs(ctx, built):
         for precise in (False, True):
             same([ctx.distance(P, Q, precise=precise, graph=True)],
                  [ctx.distance(P, Q, precise=precise)])
+
+
+def test_graph_with_phase_timing(built):
+    """Phase events recorded inside the captured graph time the replays as well."""
+    c = built.Context(0)
+    try:
+        ps = batch(built, 4)
+        Ps, Qs = [p for p, _ in ps], [q for _, q in ps]
+        c.phase_times(1)
+        want = c.distance_batch(Ps, Qs, precise=True)
+        for rep in range(2):  # capture, then replay
+            c.phase_times(1)
+            same(c.distance_batch(Ps, Qs, precise=True, graph=True), want)
+            pt = c.phase_times(1)
+            assert pt["calls"] == 1
+            assert pt["dfd_ms"] > 0 and pt["vefd_ms"] > 0 and pt["search_ms"] > 0, pt
+    finally:
+        c.close()
