@@ -269,7 +269,25 @@ __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_
 
 // Marks the boundary rows of the 32-row strips of every pair about to run `phase` as not
 // yet written (VE-FD and decision launches; see kBndEmpty).  Grid as dfd_fill_kernel.
-__global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int npairs, int phase) {
+// A gated probe round (WaveArgs.gate): the first block to look decides for the whole launch
+// whether enough pairs are still active; true to run.
+__device__ bool gate_open(int* gate, const int* active, int gate_min) {
+  int d = ld_volatile(gate);
+  if (d == 0) {
+    atomicCAS(gate, 0, ld_volatile(active) >= gate_min ? 1 : 2);
+    d = ld_volatile(gate);
+  }
+  return d == 1;
+}
+
+__global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int npairs, int phase,
+                                int* gate, const int* active, int gate_min) {
+  if (gate) {
+    __shared__ int open;
+    if (threadIdx.x == 0) open = gate_open(gate, active, gate_min);
+    __syncthreads();
+    if (!open) return;
+  }
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (int p = blockIdx.y; p < npairs; p += gridDim.y) {
     if (st[p].phase != phase || !st[p].active) continue;
@@ -323,8 +341,81 @@ __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
   }
 }
 
+// Continuous search: waits (bounded) for queue slot k to be published.  (-1, -1) when every
+// pair is done, on an error, or when the wait runs out (which sets the error word).
+__device__ int2 wait_dyn_item(const WaveArgs& wa, long long k) {
+  const long long t0 = clock64();
+  for (int it = 0;; ++it) {
+    const unsigned long long v = ld_acquire(wa.dyn_items + k);
+    if (v != ~0ull) return make_int2((int)(unsigned)(v & 0xffffffffu), (int)(unsigned)(v >> 32));
+    if ((it & 15) == 15) {
+      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error)) return make_int2(-1, -1);
+      if (clock64() - t0 > wa.spin_cycles) {
+        atomicExch(wa.error, 1);
+        return make_int2(-1, -1);
+      }
+    }
+    if (it > 64) __nanosleep(it > 1024 ? 256 : 32);
+  }
+}
+
+// Continuous search: the strips a pair keeps queued or running: wa.window, or more while
+// few pairs share the teams (one pair alone then queues its whole probe, as a launch does).
+__device__ int search_window(const WaveArgs& wa) {
+  return max(wa.window, wa.window_teams / max(1, ld_volatile(wa.active_pairs)));
+}
+
+// Continuous search: queues more strips of pair p's running probe (the next ones in strip
+// order), each in the next free slot: `count` of them, or (count = 0, called by a finishing
+// strip) at least one and enough to fill the pair's window.  The pair's lock keeps its strips
+// in strip order along the queue, so a strip's predecessor always holds an earlier ticket,
+// as in a launch's item list.  One thread.
+__device__ void push_strips(const WaveArgs& wa, PairState* st, int p, int S, int count) {
+  const long long t0 = clock64();
+  while (atomicCAS(&st->push_lock, 0, 1) != 0) {
+    if (clock64() - t0 > wa.spin_cycles || ld_volatile(wa.error)) {
+      atomicExch(wa.error, 1);
+      return;
+    }
+    __nanosleep(32);
+  }
+  __threadfence();
+  int k = *(volatile int*)&st->pushed;
+  if (count == 0)  // strips still queued or running once the caller's is done
+    count = max(1, search_window(wa) - (k - ld_volatile(&st->done_count) - 1));
+  for (int n = 0; n < count && k < S; ++n, ++k) {
+    const unsigned slot = atomicAdd(wa.dyn_tail, 1u);
+    if ((long long)slot >= wa.dyn_cap) {  // cannot happen: sized for max_probes probes per pair
+      atomicExch(wa.error, 1);
+      break;
+    }
+    st_release(wa.dyn_items + slot, ((unsigned long long)(unsigned)k << 32) | (unsigned)p);
+  }
+  *(volatile int*)&st->pushed = k;
+  __threadfence();
+  atomicExch(&st->push_lock, 0);
+}
+
+// Continuous search: the first window of strips of every pair in the search phase.
+__global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, int npairs,
+                                         WaveArgs wa) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+    if (st[p].phase != PH_SEARCH || !st[p].active) continue;
+    st[p].pushed = 0;
+    push_strips(wa, st + p, p, (pairs[p].n1 - 1 + 31) >> 5, search_window(wa));
+  }
+}
+
 // VE-FD and decision strips with the geometry computed off the dependency chain
-// (rfd_team.cuh): one CTA per strip, warp 0 propagates, warps 1..3 fill tiles.
+// (rfd_team.cuh): one CTA per strip, warp 0 propagates, warps 1..7 fill tiles.
+//
+// Continuous search (wa.dyn_items set, decisions): one launch runs every probe of every pair.
+// Strips come from a queue: each pair keeps a window of strips of its running probe queued
+// or running (a finished strip queues the next one), so pairs share the teams as they do
+// in a launch's strip-interleaved item list.  The CTA whose strip ends a pair's probe
+// clears the boundary words the probe's strips wrote (each strip records its written chunk
+// range), then queues the next probe's first strips: a pair starts its next probe as soon
+// as its last one ends, not after every pair's.
 template <int KIND>
 __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   extern __shared__ __align__(128) unsigned char team_smem[];
@@ -344,14 +435,18 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   for (;;) {
     if (threadIdx.x == 0) {
       int go = 0, quit = 0;
-      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error)) {
+      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error) ||
+          (wa.gate && ld_volatile(wa.gate) != 1)) {
         quit = 1;
       } else {
         const unsigned t = atomicAdd(wa.ticket, 1u);
-        if ((int)t >= wa.nitems) {
+        int2 it = make_int2(-1, -1);
+        if ((int)t < wa.nitems) it = wa.items[t];
+        else if (KIND == K_DEC && wa.dyn_items && (long long)t - wa.nitems < wa.dyn_cap)
+          it = wait_dyn_item(wa, (long long)t - wa.nitems);
+        if (it.x < 0) {
           quit = 1;
         } else {
-          const int2 it = wa.items[t];
           PairState* st = wa.st + it.x;
           const int S = (wa.pairs[it.x].n1 - 1 + 31) >> 5;
           if (ld_volatile(&st->phase) == wa.phase && ld_volatile(&st->active) && it.y < S) {
@@ -383,17 +478,43 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       else team_helpers<KIND, 3>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
     }
     __syncthreads();
-    if (threadIdx.x == 0 && sh->status == 0) {
-      const int S = (pd.n1 - 1 + 31) >> 5;
-      const unsigned long long ev = sh->evaluated;
-      if (ev) atomicAdd(KIND == K_DEC ? &st->cells_eval : &st->cells_vefd, ev);
-      if (KIND == K_DEC && sh->evaluated64) atomicAdd(&st->cells_fp64, sh->evaluated64);
+    const int S = (pd.n1 - 1 + 31) >> 5;
+    const bool dyn = KIND == K_DEC && wa.dyn_items != nullptr;
+    if (threadIdx.x == 0) {
+      sh->push = 0;
+      if (sh->status == 0) {
+        const unsigned long long ev = sh->evaluated;
+        if (ev) atomicAdd(KIND == K_DEC ? &st->cells_eval : &st->cells_vefd, ev);
+        if (KIND == K_DEC && sh->evaluated64) atomicAdd(&st->cells_fp64, sh->evaluated64);
+        // the probe's next strip into the window, before this strip counts as done: the
+        // probe's last strip then finds every strip queued and nothing left to queue
+        if (dyn) push_strips(wa, st, p, S, 0);
+        __threadfence();
+        const int n = atomicAdd(&st->done_count, 1);
+        if (n == S - 1) {
+          __threadfence();
+          finalize<KIND>(st, pd, wa.active_pairs);
+          __threadfence();
+          if (dyn && st->phase == PH_SEARCH && st->active) sh->push = 1;
+        }
+      }
+    }
+    __syncthreads();
+    if (KIND == K_DEC && sh->push) {
+      // the probe's written boundary words back to "not yet written", one strip per warp
+      const long long C = pd.n2 - 1;
+      for (int r = warp; r < S - 1; r += kTeamThreads / 32) {
+        const int lo = pd.prog[r].wlo, hi = pd.prog[r].whi;
+        double* row = pd.bnd + (size_t)r * pd.cstride;
+        const long long end = min((long long)(hi + 1) << 5, C);
+        for (long long w = ((long long)lo << 5) + lane; lo <= hi && w < end; w += 32)
+          reinterpret_cast<unsigned long long*>(row)[w] = kBndEmpty;
+      }
       __threadfence();
-      const int n = atomicAdd(&st->done_count, 1);
-      if (n == S - 1) {
-        __threadfence();
-        finalize<KIND>(st, pd, wa.active_pairs);
-        __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        st->pushed = 0;
+        push_strips(wa, st, p, S, search_window(wa));
       }
     }
   }
@@ -532,6 +653,9 @@ struct rfd_context {
   int grid[3] = {0, 0, 0};
   int team_grid[3] = {0, 0, 0};
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
+  int lockstep = 0;  // RFD_LOCKSTEP=1: one launch per probe round instead of the continuous search
+  int search_switch = 0;  // active pairs below which the continuous search takes over
+  int search_window = 8;  // continuous search: strips of a pair queued or running at once
   int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
   int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
   int dfd_grid[2] = {0, 0};  // [stacked, skewed] for dfd_rows
@@ -727,9 +851,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.ntitems = (int)ntitems;
   L.items = take(sizeof(int2) * nitems);
   L.titems = take(sizeof(int2) * ntitems);
-  L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0);
+  // Continuous search: a queue slot for every strip of every probe
+  // (at most 512 MB; past that, and for the solo strips, one launch per probe round)
+  int64_t dyn_cap = 0;
+  if (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo && !ctx->lockstep) {
+    for (int64_t p = 0; p < npairs; ++p)
+      dyn_cap += (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32 * max_probes;
+    if (dyn_cap * (int64_t)sizeof(unsigned long long) > ((int64_t)512 << 20)) dyn_cap = 0;
+  }
+  const size_t dyn_off = dyn_cap ? take(sizeof(unsigned long long) * dyn_cap) : 0;
+  // ticket counters: DFD, two VE-FD, probe rounds (+1 for a decision), the continuous
+  // search's ticket and queue tail; then a gate word per probe round
+  L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
   L.zero_begin = off;
-  L.counters = take(sizeof(unsigned) * L.nlaunch);
+  L.counters = take(sizeof(unsigned) * (L.nlaunch + max_probes + 1));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {  // progress words and tags: team strips only
@@ -990,7 +1125,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     prep_kernel<<<(int)std::min<int64_t>(npairs, 8 * ctx->num_sms), 256, 0, st>>>(dt, ds, (int)npairs,
                                                                                   start_phase);
     RFD_CUDA(cudaGetLastError());
-    WaveArgs wa;
+    WaveArgs wa{};
     wa.pairs = dt;
     wa.st = ds;
     wa.items = (const int2*)(dbase + L.titems);
@@ -1006,7 +1141,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
     const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
     auto fill = [&](int ph) {
-      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dt, ds, (int)npairs, ph);
+      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dt, ds, (int)npairs, ph, wa.gate,
+                                                               wa.active_pairs, wa.gate_min);
       ++launches;
     };
     if (mode != MODE_DECIDE) {
@@ -1092,7 +1228,44 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
     if (ctx->timing) RFD_CUDA(record(2));
     const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
-    for (int k = 0; k < nprobe; ++k) {
+    if (dyn_cap) {
+      // Probe rounds as single launches while many pairs are active (the rounds then keep
+      // every team busy, and a launch interleaves all pairs' strips), each skipped once
+      // fewer than search_switch remain; the continuous search finishes the rest.
+      for (int k = 0; k < nprobe; ++k) {
+        wa.phase = PH_SEARCH;
+        wa.ticket = counters + li++;
+        wa.gate = (int*)(counters + L.nlaunch + k);
+        wa.gate_min = ctx->search_switch;
+        fill(PH_SEARCH);
+        team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+        RFD_CUDA(cudaGetLastError());
+        ++launches;
+      }
+      wa.gate = nullptr;
+      // every probe of every pair in one launch: the queue starts unpublished (all ones)
+      RFD_CUDA(cudaMemsetAsync(dbase + dyn_off, 0xff, sizeof(unsigned long long) * dyn_cap, st));
+      wa.phase = PH_SEARCH;
+      wa.ticket = counters + (L.nlaunch - 2);
+      wa.dyn_items = (unsigned long long*)(dbase + dyn_off);
+      wa.dyn_tail = counters + (L.nlaunch - 1);
+      wa.dyn_cap = dyn_cap;
+      wa.window = ctx->search_window;
+      wa.window_teams = ctx->team_grid[K_DEC];
+      const int nstatic = wa.nitems;
+      wa.nitems = 0;  // every strip comes from the queue
+      fill(PH_SEARCH);
+      search_queue_init_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
+          dt, ds, (int)npairs, wa);
+      team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+      RFD_CUDA(cudaGetLastError());
+      launches += 2;
+      wa.nitems = nstatic;
+      wa.dyn_items = nullptr;
+      wa.dyn_tail = nullptr;
+      wa.dyn_cap = 0;
+    }
+    for (int k = 0; k < (dyn_cap ? 0 : nprobe); ++k) {
       wa.phase = PH_SEARCH;
       wa.ticket = counters + li++;
       if (ctx->solo) {
@@ -1120,7 +1293,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   if (use_graph) {
     const int flags[] = {mode, (int)on_device, ck, max_probes, o.stop_mode, o.reference_quirks,
                          o.dense, o.precision, o.bracket != nullptr, ctx->timing, ctx->prof,
-                         ctx->solo, ctx->dfd_rows, ctx->dfd_skew};
+                         ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
+                         ctx->search_switch, ctx->search_window};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));
@@ -1315,6 +1489,13 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     c->team_grid[K_DEC] = std::max(1, o2) * c->num_sms;
     const char* e = getenv("RFD_SOLO");
     c->solo = e && e[0] == '1';
+    const char* ls = getenv("RFD_LOCKSTEP");
+    c->lockstep = ls && ls[0] == '1';
+    c->search_switch = c->team_grid[K_DEC];  // fewer pairs than teams: rounds leave teams idle
+    const char* sw = getenv("RFD_SEARCH_SWITCH");
+    if (sw && atoi(sw) >= 0) c->search_switch = atoi(sw);
+    const char* sn = getenv("RFD_SEARCH_WINDOW");
+    if (sn && atoi(sn) >= 1) c->search_window = atoi(sn);
     const char* dr = getenv("RFD_DFD_ROWS");
     if (dr && (dr[0] == '1' || dr[0] == '2' || dr[0] == '4' || dr[0] == '8') && !dr[1])
       c->dfd_rows = dr[0] - '0';
@@ -1814,9 +1995,9 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   RFD_CUDA(cudaGetLastError());
   prep_kernel<<<1, 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH);
   RFD_CUDA(cudaGetLastError());
-  bnd_fill_kernel<<<dim3(256, 1), 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH);
+  bnd_fill_kernel<<<dim3(256, 1), 256, 0, st>>>(ddesc, dstate, 1, PH_SEARCH, nullptr, nullptr, 0);
   RFD_CUDA(cudaGetLastError());
-  WaveArgs wa;
+  WaveArgs wa{};
   wa.pairs = ddesc;
   wa.st = dstate;
   wa.items = (const int2*)(base + o_items);

@@ -35,6 +35,7 @@ struct TeamShared {
   unsigned long long evaluated;    // cells the helpers computed
   unsigned long long evaluated64;  // of those, cells with an interval computed in FP64
   int status;
+  int push;                 // continuous search: this CTA starts the pair's next probe
   int pad;
   // the strip's last row, two 32-column chunks: lane 31 stores each value as it is produced
   // (off the propagation chain), the flush reads a chunk back one column per lane
@@ -303,6 +304,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   __syncwarp();
   unsigned first_live_out = kNone;
   int next_flush = 0;
+  int wlo = INT_MAX, whi = -1;  // output chunks written (cleared before the pair's next probe)
   int pending = -1;  // chunk of the outstanding tile request (-1: none)
 
   auto request = [&](int c) {
@@ -343,6 +345,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     const double v = out_row[((k & 1) << 5) + lane];
     const bool valid = col < C;
     if (valid) st_relaxed_f64(out_bnd + col, v);
+    wlo = min(wlo, k);
+    whi = max(whi, k);
     const unsigned live = __ballot_sync(kFull, valid && !is_dead<KIND>(v, U));
     out_row[((k & 1) << 5) + lane] = dead_value<KIND>();
     __syncwarp();
@@ -660,6 +664,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       publish_cols(C);
     }
     if (!dense && lane == 0 && first_live_out == kNone) atomicMin(&st->dead_from, s + 1);
+  }
+  if (has_cons && lane == 0) {
+    out_prog->wlo = wlo;
+    out_prog->whi = whi;
   }
   if (s == S - 1 && last_row) st->result = res;
   if (wa.prof && lane == 0) atomicAdd(&wa.prof[4], (unsigned long long)(clock64() - t0));

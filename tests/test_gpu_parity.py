@@ -188,6 +188,59 @@ def test_team_equals_solo(ctx, solo_ctx, built, style, d, n1, n2):
             assert a[k] == b[k], (k, dense, a[k], b[k])
 
 
+@pytest.fixture(scope="module")
+def lockstep_ctx(built):
+    """A context that runs one launch per probe round (RFD_LOCKSTEP=1)."""
+    import os
+    old = os.environ.get("RFD_LOCKSTEP")
+    os.environ["RFD_LOCKSTEP"] = "1"
+    try:
+        c = built.Context(0)
+    finally:
+        if old is None:
+            del os.environ["RFD_LOCKSTEP"]
+        else:
+            os.environ["RFD_LOCKSTEP"] = old
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("switch", [None, "60"])
+def test_continuous_search_equals_lockstep(ctx, lockstep_ctx, built, switch):
+    """The continuous search (a pair's next probe queued as its last one ends, one launch)
+    and one launch per probe round give the same results bit for bit: every probe's
+    boundary words are cleared before the next probe reads them.  Uneven pairs, so pairs end
+    their probes at different times; with and without the learned bracket, dense, reference
+    mode, and a max_probes cap.  With the default switch (the team count) these 160 pairs
+    run continuously from the first probe; with 60, probe rounds run as launches until fewer
+    than 60 pairs are left, and the continuous search takes over mid-search."""
+    import os
+    if switch is not None:
+        os.environ["RFD_SEARCH_SWITCH"] = switch
+        try:
+            ctx = built.Context(0)
+        finally:
+            del os.environ["RFD_SEARCH_SWITCH"]
+    dims, n1, n2, styles, scales, noises = built.gen_batch_spec(2, 160, 9)
+    pairs = [built.gen_pair(int(styles[k]), int(dims[k]), min(int(n1[k]), 3000),
+                            min(int(n2[k]), 3000), float(scales[k]), float(noises[k]), 9, k)
+             for k in range(160)]
+    Ps, Qs = [a for a, _ in pairs], [b for _, b in pairs]
+    keys = ("distance", "lb", "ub", "dfd", "vefd", "probes", "flags")
+    model = built.Model.pretrained(0)
+    for kw in (dict(precise=True), dict(precise=True, model=model), dict(precise=False),
+               dict(precise=True, dense=True), dict(precise=True, max_probes=5),
+               dict(precise=True, graph=True)):
+        a = ctx.distance_batch(Ps, Qs, **kw)
+        b = lockstep_ctx.distance_batch(Ps, Qs, **kw)
+        for n, (x, y) in enumerate(zip(a, b)):
+            for k in keys:
+                assert x[k] == y[k], (kw, n, k, x[k], y[k])
+        assert max(x["probes"] for x in a) > 3
+    if switch is not None:
+        ctx.close()
+
+
 def test_reference_driver_golden(ctx, built):
     """The CUDA path in the reference's configuration reproduces the reference's own search
     driver (tests/golden/reference_host.json) bit for bit."""
