@@ -212,6 +212,9 @@ def _check(code):
 
 
 def _curve(c):
+    if (type(c) is np.ndarray and c.dtype == np.float64 and c.ndim == 2 and c.flags.c_contiguous
+            and c.shape[1] in (2, 3) and c.shape[0] >= 1):
+        return c  # already in the C ABI's layout
     a = np.ascontiguousarray(c, dtype=np.float64)
     if a.ndim != 2 or a.shape[1] not in (2, 3) or a.shape[0] < 1:
         raise ValueError("a curve is a non-empty (n, 2) or (n, 3) array")

@@ -83,8 +83,8 @@ struct PairState {
   int use_model;
   int filter;  // 1: decision intervals through the FP32 filter (RFD_PREC_FP32_FILTER)
   int coarse;  // 1: the DFD phase computes the coarse upper bound (rfd_options.coarse_ub)
-  int pushed;     // continuous search: strips of the running probe queued so far
-  int push_lock;  // continuous search: held while queueing this pair's strips
+  int pushed;      // continuous search: queue entries of the running probe so far (<= strips)
+  int next_strip;  // continuous search: strips of the running probe taken so far
 };
 
 template <int D>
@@ -104,16 +104,17 @@ struct WaveArgs {
   long long spin_cycles;
   unsigned long long* prof;  // RFD_PROF=1: cycle counters (see rfd_team.cuh), else null
   // Continuous search (team decision strips, null otherwise): tickets past nitems take the
-  // strips that pairs queue in slot ticket - nitems.
-  unsigned long long* dyn_items;  // packed (pair, strip); all ones while not published
+  // queue entry in slot ticket - nitems: a pair, whose next strip the taker then runs.
+  unsigned long long* dyn_items;  // pair index; all ones while not published
   unsigned int* dyn_tail;         // slots reserved so far
   long long dyn_cap;
   // A probe round launched ahead of the continuous search runs only while at least gate_min
-  // pairs are active; its fill kernel decides once for the launch (1: run, 2: skip).
+  // pairs, or a single one, are active; its fill kernel decides once for the launch (1: run,
+  // 2: skip).
   int* gate;
   int gate_min;
-  int window;        // continuous search: strips of a pair queued or running at once, at least
-  int window_teams;  // ... and at least this over the active pairs (few pairs: deeper chains)
+  int window;        // continuous search: strips a probe queues at its start, at least,
+  int window_teams;  // ... and at least this over the active pairs (a lone pair: its teams)
 };
 
 // ------------------------------------------------------------------ memory helpers

@@ -270,11 +270,13 @@ __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_
 // Marks the boundary rows of the 32-row strips of every pair about to run `phase` as not
 // yet written (VE-FD and decision launches; see kBndEmpty).  Grid as dfd_fill_kernel.
 // A gated probe round (WaveArgs.gate): the first block to look decides for the whole launch
-// whether enough pairs are still active; true to run.
+// whether enough pairs are still active (or a single one, which gains nothing from the
+// queue); true to run.  A skipped round does no work, so the rounds after it skip too.
 __device__ bool gate_open(int* gate, const int* active, int gate_min) {
   int d = ld_volatile(gate);
   if (d == 0) {
-    atomicCAS(gate, 0, ld_volatile(active) >= gate_min ? 1 : 2);
+    const int a = ld_volatile(active);
+    atomicCAS(gate, 0, (a >= gate_min || a == 1) ? 1 : 2);
     d = ld_volatile(gate);
   }
   return d == 1;
@@ -341,68 +343,42 @@ __global__ void __launch_bounds__(kBlock) dfd_kernel(WaveArgs wa) {
   }
 }
 
-// Continuous search: waits (bounded) for queue slot k to be published.  (-1, -1) when every
-// pair is done, on an error, or when the wait runs out (which sets the error word).
-__device__ int2 wait_dyn_item(const WaveArgs& wa, long long k) {
+// Continuous search: waits (bounded) for queue slot k to be published and returns its pair
+// index; -1 when every pair is done, on an error, or when the wait runs out (which sets the
+// error word).
+__device__ int wait_dyn_item(const WaveArgs& wa, long long k) {
   const long long t0 = clock64();
   for (int it = 0;; ++it) {
     const unsigned long long v = ld_acquire(wa.dyn_items + k);
-    if (v != ~0ull) return make_int2((int)(unsigned)(v & 0xffffffffu), (int)(unsigned)(v >> 32));
+    if (v != ~0ull) return (int)(unsigned)v;
     if ((it & 15) == 15) {
-      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error)) return make_int2(-1, -1);
+      if (ld_volatile(wa.active_pairs) == 0 || ld_volatile(wa.error)) return -1;
       if (clock64() - t0 > wa.spin_cycles) {
         atomicExch(wa.error, 1);
-        return make_int2(-1, -1);
+        return -1;
       }
     }
     if (it > 64) __nanosleep(it > 1024 ? 256 : 32);
   }
 }
 
-// Continuous search: the strips a pair keeps queued or running: wa.window, or more while
-// few pairs share the teams (one pair alone then queues its whole probe, as a launch does).
-__device__ int search_window(const WaveArgs& wa) {
-  return max(wa.window, wa.window_teams / max(1, ld_volatile(wa.active_pairs)));
+// Continuous search: the probe's counters from zero, then its first strips: wa.window, or
+// more while few pairs share the teams (a lone pair queues as many strips as there are
+// teams, as a launch's item list would).
+__device__ void start_probe(const WaveArgs& wa, PairState* st, int p, int S) {
+  st->next_strip = 0;
+  st->pushed = 0;
+  __threadfence();
+  queue_strips(wa, st, p, S,
+               max(wa.window, wa.window_teams / max(1, ld_volatile(wa.active_pairs))));
 }
 
-// Continuous search: queues more strips of pair p's running probe (the next ones in strip
-// order), each in the next free slot: `count` of them, or (count = 0, called by a finishing
-// strip) at least one and enough to fill the pair's window.  The pair's lock keeps its strips
-// in strip order along the queue, so a strip's predecessor always holds an earlier ticket,
-// as in a launch's item list.  One thread.
-__device__ void push_strips(const WaveArgs& wa, PairState* st, int p, int S, int count) {
-  const long long t0 = clock64();
-  while (atomicCAS(&st->push_lock, 0, 1) != 0) {
-    if (clock64() - t0 > wa.spin_cycles || ld_volatile(wa.error)) {
-      atomicExch(wa.error, 1);
-      return;
-    }
-    __nanosleep(32);
-  }
-  __threadfence();
-  int k = *(volatile int*)&st->pushed;
-  if (count == 0)  // strips still queued or running once the caller's is done
-    count = max(1, search_window(wa) - (k - ld_volatile(&st->done_count) - 1));
-  for (int n = 0; n < count && k < S; ++n, ++k) {
-    const unsigned slot = atomicAdd(wa.dyn_tail, 1u);
-    if ((long long)slot >= wa.dyn_cap) {  // cannot happen: sized for max_probes probes per pair
-      atomicExch(wa.error, 1);
-      break;
-    }
-    st_release(wa.dyn_items + slot, ((unsigned long long)(unsigned)k << 32) | (unsigned)p);
-  }
-  *(volatile int*)&st->pushed = k;
-  __threadfence();
-  atomicExch(&st->push_lock, 0);
-}
-
-// Continuous search: the first window of strips of every pair in the search phase.
+// Continuous search: the first strips of every pair in the search phase.
 __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, int npairs,
                                          WaveArgs wa) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
     if (st[p].phase != PH_SEARCH || !st[p].active) continue;
-    st[p].pushed = 0;
-    push_strips(wa, st + p, p, (pairs[p].n1 - 1 + 31) >> 5, search_window(wa));
+    start_probe(wa, st + p, p, (pairs[p].n1 - 1 + 31) >> 5);
   }
 }
 
@@ -410,12 +386,13 @@ __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, i
 // (rfd_team.cuh): one CTA per strip, warp 0 propagates, warps 1..7 fill tiles.
 //
 // Continuous search (wa.dyn_items set, decisions): one launch runs every probe of every pair.
-// Strips come from a queue: each pair keeps a window of strips of its running probe queued
-// or running (a finished strip queues the next one), so pairs share the teams as they do
-// in a launch's strip-interleaved item list.  The CTA whose strip ends a pair's probe
-// clears the boundary words the probe's strips wrote (each strip records its written chunk
-// range), then queues the next probe's first strips: a pair starts its next probe as soon
-// as its last one ends, not after every pair's.
+// Strips come from a queue.  A probe starts with wa.window strips queued, and each strip
+// queues one more when the band reaches it (its first live input), or when it ends without
+// live input (then every later strip is dead: it queues all of them).  A pair so keeps
+// queued about the strips its wavefront is about to need, and waiting strips hold few
+// teams.  The CTA whose strip ends a pair's probe clears the boundary words the probe's
+// strips wrote (each strip records its written chunk range), then starts the next probe: a
+// pair starts its next probe as soon as its last one ends, not after every pair's.
 template <int KIND>
 __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   extern __shared__ __align__(128) unsigned char team_smem[];
@@ -441,9 +418,12 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       } else {
         const unsigned t = atomicAdd(wa.ticket, 1u);
         int2 it = make_int2(-1, -1);
-        if ((int)t < wa.nitems) it = wa.items[t];
-        else if (KIND == K_DEC && wa.dyn_items && (long long)t - wa.nitems < wa.dyn_cap)
-          it = wait_dyn_item(wa, (long long)t - wa.nitems);
+        if ((int)t < wa.nitems) {
+          it = wa.items[t];
+        } else if (KIND == K_DEC && wa.dyn_items && (long long)t - wa.nitems < wa.dyn_cap) {
+          it.x = wait_dyn_item(wa, (long long)t - wa.nitems);
+          if (it.x >= 0) it.y = atomicAdd(&wa.st[it.x].next_strip, 1);
+        }
         if (it.x < 0) {
           quit = 1;
         } else {
@@ -458,6 +438,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       }
       sh->go = go;
       sh->quit = quit;
+      sh->push_req = 0;
       sh->evaluated = 0ull;
       sh->evaluated64 = 0ull;
       sh->status = 0;
@@ -486,9 +467,10 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
         const unsigned long long ev = sh->evaluated;
         if (ev) atomicAdd(KIND == K_DEC ? &st->cells_eval : &st->cells_vefd, ev);
         if (KIND == K_DEC && sh->evaluated64) atomicAdd(&st->cells_fp64, sh->evaluated64);
-        // the probe's next strip into the window, before this strip counts as done: the
-        // probe's last strip then finds every strip queued and nothing left to queue
-        if (dyn) push_strips(wa, st, p, S, 0);
+        // the strip's queue entry if its band start did not queue it (all the rest for a
+        // strip without live input), before the strip counts as done: the probe's last
+        // strip then finds every strip queued
+        if (dyn && sh->push_req != 2) queue_strips(wa, st, p, S, sh->push_req == 3 ? S : 1);
         __threadfence();
         const int n = atomicAdd(&st->done_count, 1);
         if (n == S - 1) {
@@ -512,10 +494,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       }
       __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) {
-        st->pushed = 0;
-        push_strips(wa, st, p, S, search_window(wa));
-      }
+      if (threadIdx.x == 0) start_probe(wa, st, p, S);
     }
   }
 }
@@ -655,7 +634,7 @@ struct rfd_context {
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
   int lockstep = 0;  // RFD_LOCKSTEP=1: one launch per probe round instead of the continuous search
   int search_switch = 0;  // active pairs below which the continuous search takes over
-  int search_window = 8;  // continuous search: strips of a pair queued or running at once
+  int search_window = 2;  // continuous search: strips a probe queues ahead of its band
   int dfd_rows = 8;    // rows per lane of the DFD strips (RFD_DFD_ROWS = 1, 2, 4 or 8)
   int dfd_skew = -1;   // RFD_DFD_SKEW: 1 skewed rows, 0 stacked, unset: chosen per call
   int dfd_grid[2] = {0, 0};  // [stacked, skewed] for dfd_rows

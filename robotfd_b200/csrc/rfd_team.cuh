@@ -36,11 +36,29 @@ struct TeamShared {
   unsigned long long evaluated64;  // of those, cells with an interval computed in FP64
   int status;
   int push;                 // continuous search: this CTA starts the pair's next probe
-  int pad;
+  int push_req;             // continuous search: 1 the strip's band started (queue a strip),
+                            // 2 queued, 3 the strip found no live input (queue the rest)
   // the strip's last row, two 32-column chunks: lane 31 stores each value as it is produced
   // (off the propagation chain), the flush reads a chunk back one column per lane
   double out_row[64];
 };
+
+// Continuous search: makes `count` more strips of pair p's running probe available (S per
+// probe at most), one queue entry, the pair's index, each.  A taker draws the strip index
+// from the pair's next_strip counter, so strips start in order and a strip's predecessor is
+// always already running, as with a launch's item list.  One thread.
+__device__ __forceinline__ void queue_strips(const WaveArgs& wa, PairState* st, int p, int S,
+                                             int count) {
+  const int k = atomicAdd(&st->pushed, count);
+  const int n = min(count, S - k);
+  if (n <= 0) return;
+  const unsigned slot = atomicAdd(wa.dyn_tail, (unsigned)n);
+  if ((long long)slot + n > wa.dyn_cap) {  // cannot happen: sized for max_probes probes per pair
+    atomicExch(wa.error, 1);
+    return;
+  }
+  for (int i = 0; i < n; ++i) st_release(wa.dyn_items + slot + i, (unsigned long long)(unsigned)p);
+}
 
 // Column records of one tile, staged by the helpers: the tile of step-chunk c reads the
 // columns c*32-31 .. c*32+31, i.e. the points q_{c*32-31} .. q_{c*32+32} and the segments'
@@ -228,6 +246,13 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     __syncwarp();
     if (lane == 0) mbar_arrive(&sh->full[slot]);
     ++seqH;
+    if (wa.dyn_items && hw == 0 && lane == 0 && *(volatile int*)&sh->push_req == 1) {
+      // the band reached this strip: queue one more of the probe, once this warp's share of
+      // the tile is in (the push's round trips then delay no tile)
+      *(volatile int*)&sh->push_req = 2;
+      PairState* ps = const_cast<PairState*>(st);
+      queue_strips(wa, ps, (int)(ps - wa.st), (R + 31) >> 5, 1);
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -462,6 +487,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
     if (in_live && !seen_live) {
       seen_live = true;
+      // the band reached this strip: a helper queues one more strip of the probe
+      if (wa.dyn_items && lane == 0) *(volatile int*)&sh->push_req = 1;
       // Liveness enters a strip only through its input row, so no output chunk before c can
       // be live: publish c as a lower bound of the first live output chunk (the flush of the
       // actual one overwrites it), so the next strip moves to this strip's band and starts
@@ -663,7 +690,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     } else {
       publish_cols(C);
     }
-    if (!dense && lane == 0 && first_live_out == kNone) atomicMin(&st->dead_from, s + 1);
+    if (!dense && lane == 0 && first_live_out == kNone) {
+      atomicMin(&st->dead_from, s + 1);
+      if (wa.dyn_items) *(volatile int*)&sh->push_req = 3;  // every later strip is dead too
+    }
   }
   if (has_cons && lane == 0) {
     out_prog->wlo = wlo;
