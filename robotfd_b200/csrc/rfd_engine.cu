@@ -386,9 +386,9 @@ __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, i
 // (rfd_team.cuh): one CTA per strip, warp 0 propagates, warps 1..7 fill tiles.
 //
 // Continuous search (wa.dyn_items set, decisions): one launch runs every probe of every pair.
-// Strips come from a queue.  A probe starts with wa.window strips queued, and each strip
-// queues one more when the band reaches it (its first live input), or when it ends without
-// live input (then every later strip is dead: it queues all of them).  A pair so keeps
+// Strips come from a queue.  A probe starts with a few strips queued (start_probe), and
+// each strip queues one more when the band reaches it (its first live input), or when it ends
+// without live input (then every later strip is dead: it queues all of them).  A pair so keeps
 // queued about the strips its wavefront is about to need, and waiting strips hold few
 // teams.  The CTA whose strip ends a pair's probe clears the boundary words the probe's
 // strips wrote (each strip records its written chunk range), then starts the next probe: a
