@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--profile-batch", type=int, default=0, metavar="N",
                     help="profiling case: one batched call (one probe) on the first N pairs of "
                          "the uneven batch, then exit (no JSON line)")
+    ap.add_argument("--profile-search", type=int, default=0, metavar="N",
+                    help="profiling case: one batched call of the learned form (every probe) on "
+                         "the first N pairs of the uneven batch, then exit (no JSON line)")
     return ap.parse_args()
 
 
@@ -326,6 +329,13 @@ def main():
         pairs = batch_pairs()[: args.profile_batch]
         ctx = rfd.Context(0)
         ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True, max_probes=1)
+        ctx.close()
+        return
+    if args.profile_search:
+        pairs = batch_pairs()[: args.profile_search]
+        ctx = rfd.Context(0)
+        ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True,
+                           model=rfd.Model.pretrained(0))
         ctx.close()
         return
 
