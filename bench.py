@@ -244,6 +244,8 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
     mixed = dict(batched, precision=rfd.RFD_PREC_FP32_FILTER)
     ctx.distance_batch(Ps, Qs, **mixed)
     t_m, learned_mixed = timed(lambda: ctx.distance_batch(Ps, Qs, **mixed), 2)
+    # untimed first call: the coarse pairs' arrays can grow the context's workspace once
+    ctx.distance_batch(Ps, Qs, precise=True, model=model, coarse_ub=COARSE_UB)
     t_c, _ = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
                                               coarse_ub=COARSE_UB), 1)
     t_p, plain = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True), 1)
