@@ -85,7 +85,9 @@ typedef struct rfd_options {
                                bound (RFD_FLAG_DFD_COARSE).  The FD, within the stop rule, does
                                not depend on it. */
   int32_t drop_repeats;     /* 1: drop consecutive repeated points (all coordinates equal) from
-                               both curves before the solve (host memory only).  The Frechet
+                               both curves before the solve (device-memory curves are counted
+                               and compacted on the device, with one read-back of the counts
+                               before the call's launches).  The Frechet
                                distance does not change in exact arithmetic, but the reference's
                                free interval of a zero-length segment is [0, 1] at every radius
                                (src/intersection_algorithm_in_parallel.cu:1186-1198: 0 * inf is

@@ -250,6 +250,76 @@ __global__ void coarse_prep_kernel(const PairDesc* pairs, const PairDesc* coarse
   }
 }
 
+// drop_repeats on device-memory curves (rfd_options.drop_repeats): point k is kept unless
+// every coordinate equals point k-1's, as same_point on the host.
+struct SrcCurve {
+  const double* src;  // the caller's curve
+  double* dst;        // its kept points, in the workspace
+  long long n;        // the caller's point count
+  int d, pad;
+};
+__device__ __forceinline__ bool same_point_dev(const double* a, const double* b, int d) {
+  for (int e = 0; e < d; ++e)
+    if (!(a[e] == b[e])) return false;
+  return true;
+}
+
+// Points kept per curve.  One block of 256 per curve (grid-stride).
+__global__ void __launch_bounds__(256) count_kept_kernel(const SrcCurve* cs, int ncurves,
+                                                         long long* kept) {
+  __shared__ long long part[8];
+  for (int c = blockIdx.x; c < ncurves; c += gridDim.x) {
+    const SrcCurve sc = cs[c];
+    long long m = 0;
+    for (long long k = 1 + threadIdx.x; k < sc.n; k += blockDim.x)
+      m += !same_point_dev(sc.src + (k - 1) * sc.d, sc.src + k * sc.d, sc.d);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m += __shfl_xor_sync(kFull, m, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long t = sc.n > 0 ? 1 : 0;
+      for (int w = 0; w < 8; ++w) t += part[w];
+      kept[c] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// The kept points, in order, into the workspace: tiles of 256 points, each point's place the
+// tile's running count plus a block scan of the keep flags.  One block of 256 per curve.
+__global__ void __launch_bounds__(256) compact_kept_kernel(const SrcCurve* cs, int ncurves) {
+  __shared__ int warp_tot[8];
+  __shared__ long long base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = blockIdx.x; c < ncurves; c += gridDim.x) {
+    const SrcCurve sc = cs[c];
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (long long t0 = 0; t0 < sc.n; t0 += 256) {
+      const long long k = t0 + threadIdx.x;
+      const bool keep =
+          k < sc.n && (k == 0 || !same_point_dev(sc.src + (k - 1) * sc.d, sc.src + k * sc.d, sc.d));
+      const unsigned b = __ballot_sync(kFull, keep);
+      if (lane == 0) warp_tot[warp] = __popc(b);
+      __syncthreads();
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += warp_tot[w];
+      if (keep) {
+        const long long at = base + before + __popc(b & ((1u << lane) - 1u));
+        for (int e = 0; e < sc.d; ++e) sc.dst[at * sc.d + e] = sc.src[k * sc.d + e];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int w = 0; w < 8; ++w) tot += warp_tot[w];
+        base += tot;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Marks the rows the DFD strips of 32*K rows hand to each other as not yet written (the
 // all-ones pattern, a NaN no DFD value takes).  Pairs are spread over grid rows (y) and
 // each pair's rows over grid columns (x), so one large pair uses every SM.
@@ -775,13 +845,43 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   const int64_t* const in_n2s = n2s;
   std::vector<int64_t> kept1, kept2;
   const bool drop = mode == MODE_DISTANCE && o.drop_repeats;
+  // device-memory curves with drop_repeats are compacted into the workspace on the device
+  const bool dcompact = drop && on_device;
   if (drop) {
-    if (on_device) return fail(RFD_ERR_ARG, "drop_repeats needs curves in host memory");
     kept1.resize(npairs);
     kept2.resize(npairs);
-    for (int64_t p = 0; p < npairs; ++p) {
-      kept1[p] = kept_points(c1s[p], n1s[p], dims[p]);
-      kept2[p] = kept_points(c2s[p], n2s[p], dims[p]);
+    if (on_device) {
+      // the kept counts size the layout: counted on the device, read back before it
+      const size_t nb = align_up(sizeof(SrcCurve) * 2 * npairs, 256);
+      const size_t kb = sizeof(long long) * 2 * npairs;
+      int rc0 = ensure_device(ctx, nb + kb);
+      if (rc0) return rc0;
+      rc0 = ensure_host(ctx, nb + kb);
+      if (rc0) return rc0;
+      SrcCurve* hsc = (SrcCurve*)ctx->hws;
+      for (int64_t p = 0; p < npairs; ++p) {
+        hsc[2 * p] = SrcCurve{c1s[p], nullptr, (long long)n1s[p], dims[p], 0};
+        hsc[2 * p + 1] = SrcCurve{c2s[p], nullptr, (long long)n2s[p], dims[p], 0};
+      }
+      RFD_CUDA(cudaMemcpyAsync(ctx->dws, ctx->hws, sizeof(SrcCurve) * 2 * npairs,
+                               cudaMemcpyHostToDevice, ctx->stream));
+      count_kept_kernel<<<(int)std::min<int64_t>(2 * npairs, 8 * ctx->num_sms), 256, 0,
+                          ctx->stream>>>((const SrcCurve*)ctx->dws, (int)(2 * npairs),
+                                         (long long*)((char*)ctx->dws + nb));
+      RFD_CUDA(cudaGetLastError());
+      RFD_CUDA(cudaMemcpyAsync((char*)ctx->hws + nb, (char*)ctx->dws + nb, kb,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+      RFD_CUDA(cudaStreamSynchronize(ctx->stream));
+      const long long* kc = (const long long*)((char*)ctx->hws + nb);
+      for (int64_t p = 0; p < npairs; ++p) {
+        kept1[p] = kc[2 * p];
+        kept2[p] = kc[2 * p + 1];
+      }
+    } else {
+      for (int64_t p = 0; p < npairs; ++p) {
+        kept1[p] = kept_points(c1s[p], n1s[p], dims[p]);
+        kept2[p] = kept_points(c2s[p], n2s[p], dims[p]);
+      }
     }
     n1s = kept1.data();
     n2s = kept2.data();
@@ -860,12 +960,13 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // host curves: one contiguous region laid out exactly as the pinned staging area below
   // (same sizes, same 256-byte alignment), so a single copy moves every curve
   const size_t curves_begin = off;
-  if (!on_device)
+  if (!on_device || dcompact)
     for (int64_t p = 0; p < npairs; ++p) {
       L.P[p] = take(sizeof(double) * n1s[p] * dims[p]);
       L.Q[p] = take(sizeof(double) * n2s[p] * dims[p]);
     }
   const size_t curves_end = off;
+  const size_t src_off = dcompact ? take(sizeof(SrcCurve) * 2 * npairs) : 0;
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
     const int d = dims[p];
@@ -898,6 +999,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.h_items = htake(sizeof(int2) * nitems);
   L.h_titems = htake(sizeof(int2) * ntitems);
   L.h_misc = htake(4 * sizeof(int));
+  const size_t h_src = dcompact ? htake(sizeof(SrcCurve) * 2 * npairs) : 0;
   L.h_curves = hoff;
   if (!on_device) {
     for (int64_t p = 0; p < npairs; ++p) {
@@ -924,12 +1026,17 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int64_t S = (n1 + 31) / 32;
     PairDesc& D = hd[p];
     memset(&D, 0, sizeof(D));
-    if (on_device) {
+    if (on_device && !dcompact) {
       D.P = c1s[p];
       D.Q = c2s[p];
-    } else {  // staged below
+    } else {  // staged below, or compacted on the device
       D.P = (const double*)(dbase + L.P[p]);
       D.Q = (const double*)(dbase + L.Q[p]);
+    }
+    if (dcompact) {
+      SrcCurve* hsc = (SrcCurve*)(hbase + h_src);
+      hsc[2 * p] = SrcCurve{c1s[p], (double*)(dbase + L.P[p]), (long long)in_n1s[p], d, 0};
+      hsc[2 * p + 1] = SrcCurve{c2s[p], (double*)(dbase + L.Q[p]), (long long)in_n2s[p], d, 0};
     }
     D.rowc = (const double2*)(dbase + L.rowc[p]);
     D.colrec = (const double2*)(dbase + L.colrec[p]);
@@ -1086,6 +1193,16 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                              cudaMemcpyHostToDevice, st));
     RFD_CUDA(cudaMemcpyAsync(dbase + L.titems, hbase + L.h_titems, sizeof(int2) * ntitems,
                              cudaMemcpyHostToDevice, st));
+    if (dcompact) {
+      // the caller's curves (pointers refreshed every call) compacted into the workspace
+      RFD_CUDA(cudaMemcpyAsync(dbase + src_off, hbase + h_src, sizeof(SrcCurve) * 2 * npairs,
+                               cudaMemcpyHostToDevice, st));
+      h2d_bytes += sizeof(SrcCurve) * 2 * npairs;
+      compact_kept_kernel<<<(int)std::min<int64_t>(2 * npairs, 8 * ctx->num_sms), 256, 0, st>>>(
+          (const SrcCurve*)(dbase + src_off), (int)(2 * npairs));
+      RFD_CUDA(cudaGetLastError());
+      ++launches;
+    }
     if (!on_device && curves_end > curves_begin) {
       // the device curve region mirrors the staging area byte for byte: one copy
       RFD_CUDA(cudaMemcpyAsync(dbase + curves_begin, hbase + L.h_curves, curves_end - curves_begin,
@@ -1270,7 +1387,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     for (size_t i = 0; i < n; ++i) key = (key ^ b[i]) * 1099511628211ull;
   };
   if (use_graph) {
-    const int flags[] = {mode, (int)on_device, ck, max_probes, o.stop_mode, o.reference_quirks,
+    const int flags[] = {mode, (int)on_device, (int)drop, ck, max_probes, o.stop_mode, o.reference_quirks,
                          o.dense, o.precision, o.bracket != nullptr, ctx->timing, ctx->prof,
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
                          ctx->search_switch, ctx->search_window};

@@ -158,8 +158,43 @@ def test_drop_repeats_batch(ctx, built):
             assert any(a["distance"] < b["distance"] for a, b in zip(plain, got))
 
 
-def test_drop_repeats_needs_host_curves(ctx, built):
+def test_drop_repeats_on_device_curves(ctx, built):
+    """Device-memory curves are counted and compacted on the device: the results equal the
+    host path's bit for bit, single pairs and batches, and a replayed CUDA graph reads the
+    new call's curves."""
     import torch
-    P = torch.zeros((4, 2), dtype=torch.float64, device="cuda")
-    with pytest.raises(built.RfdError):
-        ctx.distance_device(P.data_ptr(), 4, P.data_ptr(), 4, 2, drop_repeats=True)
+    rng = np.random.default_rng(7)
+    ps = []
+    for k in range(10):
+        d = 2 + k % 2
+        P = with_repeats(rng, np.cumsum(rng.normal(size=(int(rng.integers(2, 700)), d)), 0))
+        Q = with_repeats(rng, np.cumsum(rng.normal(size=(int(rng.integers(2, 700)), d)), 0))
+        ps.append((P, Q))
+    ps.append((np.repeat([[1.0, 2.0]], 5, axis=0), ps[0][1]))  # a curve of one repeated point
+    ps.append((np.array([[0.5, 0.5]]), ps[2][1]))               # a one-point curve
+    keys = ("distance", "lb", "ub", "dfd", "vefd", "endpoint", "probes", "cells_nominal", "flags")
+    dev = [(torch.tensor(P, device="cuda"), torch.tensor(Q, device="cuda")) for P, Q in ps]
+    for precise in (False, True):
+        want = ctx.distance_batch([P for P, _ in ps], [Q for _, Q in ps], precise=precise,
+                                  drop_repeats=True)
+        for (P, Q), (a, b), w in zip(ps, dev, want):
+            got = ctx.distance_device(a.data_ptr(), len(P), b.data_ptr(), len(Q), P.shape[1],
+                                      precise=precise, drop_repeats=True)
+            for key in keys:
+                assert got[key] == w[key], (key, got[key], w[key])
+        batch = ctx.distance_batch([(a.data_ptr(), len(P), P.shape[1]) for (P, _), (a, _) in zip(ps, dev)],
+                                   [(b.data_ptr(), len(Q), Q.shape[1]) for (_, Q), (_, b) in zip(ps, dev)],
+                                   precise=precise, drop_repeats=True, memory=built.RFD_MEM_DEVICE)
+        for g, w in zip(batch, want):
+            for key in keys:
+                assert g[key] == w[key], (key, g[key], w[key])
+    # graph replay: same kept sizes, other coordinates in other device buffers
+    P, Q = ps[3]
+    a, b = dev[3]
+    kw = dict(precise=True, drop_repeats=True, memory=built.RFD_MEM_DEVICE, graph=True)
+    first = ctx.distance_batch([(a.data_ptr(), len(P), P.shape[1])], [(b.data_ptr(), len(Q), Q.shape[1])], **kw)
+    assert first[0]["distance"] == ctx.distance(P, Q, precise=True, drop_repeats=True)["distance"]
+    P2, Q2 = P * 1.5 + 0.25, Q * 0.75
+    a2, b2 = torch.tensor(P2, device="cuda"), torch.tensor(Q2, device="cuda")
+    again = ctx.distance_batch([(a2.data_ptr(), len(P2), P2.shape[1])], [(b2.data_ptr(), len(Q2), Q2.shape[1])], **kw)
+    assert again[0]["distance"] == ctx.distance(P2, Q2, precise=True, drop_repeats=True)["distance"]
