@@ -136,15 +136,44 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(points=200000):
-    """The long pair; other sizes keep its generator (waypoints = points / 100, seed 1)."""
-    import robotfd_b200 as rfd
+def workload(points=200000, gen=None):
+    """The long pair; other sizes keep its generator (waypoints = points / 100, seed 1).
+    gen: the module whose seeded generator makes it (the CPU arm passes the oracle, which
+    carries a copy of the same generator, so that it never loads librfd.so)."""
+    if gen is None:
+        import robotfd_b200 as gen
     if points == 200000:
-        return rfd.gen_config(1)[0]
-    return rfd.gen_pair(1, 3, points, points, 100.0, 0.1, 1, 0)
+        return gen.gen_config(1)[0]
+    return gen.gen_pair(1, 3, points, points, 100.0, 0.1, 1, 0)
 
 
-def cpu_sample(P, Q, m, probes):
+GOLDENS = os.path.join(ROOT, "tests", "golden", "config_goldens.json")
+
+
+def workload_probes(P, Q, points):
+    """Decisions of the plain method's solve of the workload at 2^-33, as the CPU oracle made
+    them: the committed golden of the long pair, or (other sizes) an oracle solve."""
+    import oracle
+    if points == 200000 and os.path.exists(GOLDENS):
+        with open(GOLDENS) as f:
+            rec = json.load(f)["cases"].get("config1/0")
+        if rec:
+            return rec["probes"], "oracle golden of this pair (tests/golden/config_goldens.json)"
+    r = oracle.distance(P, Q, stop_mode=1, quirks=False, threads=oracle.max_threads())
+    return r["probes"], "oracle solve of this pair"
+
+
+def config_dict(points, n1, n2, d, world):
+    """The workload description both arms print (same keys and values)."""
+    return {"workload": WORKLOAD if points == 200000 else
+            f"long-pair generator at {points} points per curve", "n1": n1, "n2": n2,
+            "dims": d, "stop": "ub-lb <= 2^-33 ub",
+            "form": f"learned bracket (shipped network), coarse upper bound k={COARSE_UB}",
+            "parallelism": f"replicas x{world}",
+            "l2": "flushed before every step (256 MiB write outside the timed events)"}
+
+
+def cpu_sample(P, Q, m, probes, probes_src="the plain method's decisions"):
     """Dense CPU oracle on the first m points of each curve: DFD, VE-FD and one decision,
     timed; the rates extrapolate to one solve of the full pair with `probes` decisions."""
     import oracle
@@ -166,21 +195,42 @@ def cpu_sample(P, Q, m, probes):
         "value": 1.0 / sec, "unit": "solves/s", "cores": threads, "kind": "port",
         "sample": (f"oracle (dense FP64, OpenMP {threads} threads): DFD, VE-FD and one decision "
                    f"on the first {m} points of each curve ({t3 - t0:.1f} s), extrapolated to "
-                   f"the full pair with {probes} decisions"),
+                   f"the full pair with {probes} decisions ({probes_src})"),
         "cells_per_s": {"dfd": r_dfd, "vefd": r_ve, "decision": r_dec},
     }
 
 
+def cpu_batch_sample(every=64):
+    """Measured, not extrapolated: the CPU oracle fully solves (plain method, 2^-33) every
+    `every`-th pair of the uneven batch, one pair after another on all host threads."""
+    import oracle
+    threads = oracle.max_threads()
+    dims, n1, n2, styles, scales, noises = oracle.gen_batch_spec(2, 4096, 2)
+    idx = list(range(0, 4096, every))
+    pairs = [oracle.gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]),
+                             float(scales[k]), float(noises[k]), 2, k) for k in idx]
+    t0 = time.perf_counter()
+    res = [oracle.distance(p, q, stop_mode=1, quirks=False, threads=threads) for p, q in pairs]
+    sec = time.perf_counter() - t0
+    return {"value": len(idx) / sec, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(idx)} pairs of the 4096-pair batch (every {every}th), each fully "
+                      f"solved by the oracle (dense FP64, OpenMP), {sec:.1f} s",
+            "mean_probes": statistics.mean(r["probes"] for r in res)}
+
+
 def reference_arm(args):
-    """CPU implementation of the path (the oracle port: the reference has no CPU path)."""
+    """CPU implementation of the path (the oracle port: the reference has no CPU path).
+    Imports only the oracle (inputs from its copy of the generator): librfd.so stays
+    unloaded in this arm."""
+    import oracle
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    P, Q = workload(args.points)
-    probes = 37  # decisions of this workload's solve at 2^-33 (identical decisions as the GPU)
+    P, Q = workload(args.points, gen=oracle)
+    probes, src = workload_probes(P, Q, args.points)
     vals = []
     for k in range(args.warmup + args.steps):
-        r = cpu_sample(P, Q, args.cpu_sample, probes)
+        r = cpu_sample(P, Q, args.cpu_sample, probes, src)
         if k >= args.warmup:
             vals.append(r["value"])
     v = statistics.median(vals)
@@ -188,7 +238,8 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "cpu"},
+            "data": "synthetic",
+            "config": config_dict(args.points, len(P), len(Q), P.shape[1], world),
             "cpu_baseline": r,
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -467,12 +518,7 @@ def main():
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.points == 200000 else
-                   f"long-pair generator at {args.points} points per curve", "n1": n1, "n2": n2,
-                   "dims": d, "stop": "ub-lb <= 2^-33 ub",
-                   "form": f"learned bracket (shipped network), coarse upper bound k={COARSE_UB}",
-                   "parallelism": f"replicas x{world}",
-                   "l2": "flushed before every step (256 MiB write outside the timed events)"},
+        "config": config_dict(args.points, n1, n2, d, world),
         "fd": res["distance"],
         "dfd": res["dfd"],
         "vefd": res["vefd"],
@@ -518,7 +564,13 @@ def main():
         line["mixed_precision"] = mixed_leg(ctx, model, timed, args.mixed_pairs)
     if rank == 0:
         if world == 1:
-            line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, pres["probes"])
+            probes, src = workload_probes(P, Q, args.points)
+            line["cpu_baseline"] = cpu_sample(P, Q, args.cpu_sample, probes, src)
+            if "batch" in line:
+                line["batch"]["cpu_measured"] = cpu_batch_sample()
+                line["batch"]["learned_batched_vs_cpu_measured"] = (
+                    line["batch"]["solves_per_s"]["learned_batched"] /
+                    line["batch"]["cpu_measured"]["value"])
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

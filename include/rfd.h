@@ -132,6 +132,14 @@ void rfd_options_init(rfd_options* opt, int32_t precise);
 /* ---- context ---- */
 int32_t rfd_context_create(int32_t device, rfd_context** out);
 int32_t rfd_context_destroy(rfd_context* ctx);
+/* Budget of every bounded wait of the context's kernels (a strip waiting for the strip above
+   it, a helper warp for its request, the continuous search for a queue entry), in SM clock
+   cycles; cycles <= 0 restores the default of about 20 s at the maximum SM clock.  A wait that
+   runs out sets an error word, every warp leaves, and the call returns RFD_ERR_TIMEOUT; the next
+   call starts afresh.  The environment variable RFD_SPIN_CYCLES sets the initial budget of new
+   contexts and the budget of rfd_decide_noalloc.  (The reference's spin-waits are unbounded,
+   src/intersection_algorithm_in_parallel.cu:304-306, :332-334.) */
+int32_t rfd_context_set_wait_budget(rfd_context* ctx, int64_t cycles);
 /* Use a caller stream (cudaStream_t) instead of the context's own; NULL restores it. */
 int32_t rfd_context_set_stream(rfd_context* ctx, void* stream);
 /* Phase timing with CUDA events on the context's stream (off by default; no reference
@@ -205,8 +213,11 @@ int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double*
    memory is one file-scope device array of 64 MiB that every GPU loading librfd.so holds
    until exit (pairs needing more return RFD_ERR_LIMIT before anything runs).  The work is
    enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the call returns
-   without waiting: *right_ub receives the propagated right UB of the last cell (reachable
-   iff it equals 1.0), or NaN if an inter-warp wait timed out.  The first call on a device
+   without waiting, so its status covers the arguments and the enqueueing only: what the
+   kernels find arrives in *right_ub.  It receives the propagated right UB of the last cell
+   (reachable iff it equals 1.0), a value in [-2, 1], or NaN when an inter-warp wait ran out
+   of its budget (RFD_SPIN_CYCLES, else about 20 s): NaN means the decision failed and must
+   not be read as "not reachable"; the next call starts afresh.  The first call on a device
    looks up the array's address and sets kernel attributes there, so make that first call
    before any stream capture.  All calls share the array and each clears what must start
    at zero; calls whose work overlaps on the GPU race and must not be issued. */

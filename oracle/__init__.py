@@ -57,6 +57,12 @@ def lib():
         L.rfd_verify_free_bounds.argtypes = [_dp, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp]
         L.rfd_oracle_free_intervals.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, ctypes.c_double,
                                                 ctypes.c_int, _dp, _dp]
+        L.rfd_oracle_gen_pair.argtypes = [ctypes.c_int, ctypes.c_int, i64, i64, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _dp,
+                                          ctypes.POINTER(i64), _dp, ctypes.POINTER(i64)]
+        L.rfd_oracle_gen_batch_spec.argtypes = [ctypes.c_int, i64, ctypes.c_uint64, _ip,
+                                                ctypes.POINTER(i64), ctypes.POINTER(i64), _ip,
+                                                _dp, _dp]
         _LIB = L
     return _LIB
 
@@ -183,3 +189,55 @@ def verify_free_bounds(x, s, e, radius):
     out = (ctypes.c_double * 4)()
     lib().rfd_verify_free_bounds(_ptr(x), _ptr(s), _ptr(e), float(radius), len(x), out)
     return (out[0], out[1]), (out[2], out[3])
+
+
+# ---- seeded workloads (the same generator source as librfd's, compiled into this library,
+# so that the CPU baseline makes its inputs without loading the product)
+def gen_pair(style, dims, n1, n2, scale, noise, seed, stream=0):
+    P = np.empty((n1, dims))
+    Q = np.empty((n2, dims))
+    m1, m2 = ctypes.c_int64(), ctypes.c_int64()
+    rc = lib().rfd_oracle_gen_pair(style, dims, n1, n2, scale, noise, seed, stream, _ptr(P),
+                                   ctypes.byref(m1), _ptr(Q), ctypes.byref(m2))
+    if rc:
+        raise RuntimeError(f"oracle gen_pair failed ({rc})")
+    return P[: m1.value].copy(), Q[: m2.value].copy()
+
+
+def gen_batch_spec(config, npairs, seed):
+    dims = np.empty(npairs, np.int32)
+    n1 = np.empty(npairs, np.int64)
+    n2 = np.empty(npairs, np.int64)
+    styles = np.empty(npairs, np.int32)
+    scales = np.empty(npairs)
+    noises = np.empty(npairs)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    rc = lib().rfd_oracle_gen_batch_spec(config, npairs, seed, dims.ctypes.data_as(_ip),
+                                         n1.ctypes.data_as(i64p), n2.ctypes.data_as(i64p),
+                                         styles.ctypes.data_as(_ip), _ptr(scales), _ptr(noises))
+    if rc:
+        raise RuntimeError(f"oracle gen_batch_spec failed ({rc})")
+    return dims, n1, n2, styles, scales, noises
+
+
+CONFIG_DEFAULTS = {0: (1, 0), 1: (1, 1), 2: (4096, 2), 3: (200000, 3), 4: (512, 5)}
+
+
+def gen_config_pair(config, k, seed=None):
+    """Pair k of a benchmark workload (see gen_config)."""
+    seed = CONFIG_DEFAULTS[config][1] if seed is None else seed
+    dims, n1, n2, styles, scales, noises = gen_batch_spec(config, k + 1, seed)
+    return gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]), float(scales[k]),
+                    float(noises[k]), seed, k)
+
+
+def gen_config(config, npairs=None, seed=None):
+    """Pairs of a benchmark workload: 0 walk 2000x1900 2D (seed 0), 1 spline 200k x 200k 3D
+    (seed 1), 2 4096 uneven pairs (seed 2), 3 training pairs (seed 3), 4 512 large 3D pairs
+    (seed 5).  Returns a list of (P, Q)."""
+    dn, ds = CONFIG_DEFAULTS[config]
+    npairs = dn if npairs is None else npairs
+    seed = ds if seed is None else seed
+    dims, n1, n2, styles, scales, noises = gen_batch_spec(config, npairs, seed)
+    return [gen_pair(int(styles[k]), int(dims[k]), int(n1[k]), int(n2[k]), float(scales[k]),
+                     float(noises[k]), seed, k) for k in range(npairs)]

@@ -50,6 +50,7 @@ REL_TOL = 2.0 ** -33
 EXPORTS = (
     "rfd_abi_version", "rfd_status_string", "rfd_last_error", "rfd_options_init",
     "rfd_context_create", "rfd_context_destroy", "rfd_context_set_stream",
+    "rfd_context_set_wait_budget",
     "rfd_context_phase_times", "rfd_fp64_peak", "rfd_distance",
     "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_load_txt", "rfd_free",
     "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
@@ -135,6 +136,8 @@ def lib():
     L.rfd_context_destroy.restype = i32
     L.rfd_context_set_stream.argtypes = [vp, vp]
     L.rfd_context_set_stream.restype = i32
+    L.rfd_context_set_wait_budget.argtypes = [vp, ctypes.c_int64]
+    L.rfd_context_set_wait_budget.restype = i32
     L.rfd_context_phase_times.argtypes = [vp, i32, _dp]
     L.rfd_context_phase_times.restype = i32
     L.rfd_fp64_peak.argtypes = [vp, _dp]
@@ -262,6 +265,10 @@ class Context:
 
     def set_stream(self, stream_handle):
         _check(lib().rfd_context_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def set_wait_budget(self, cycles=0):
+        """Budget of every bounded wait in SM clock cycles (<= 0: the default, about 20 s)."""
+        _check(lib().rfd_context_set_wait_budget(self._h, int(cycles)))
 
     def phase_times(self, enable=-1):
         """Per-phase device ms since the last query: dict(dfd, vefd, search, calls, launches)."""

@@ -715,7 +715,8 @@ struct rfd_context {
   size_t dws_size = 0;
   void* hws = nullptr;
   size_t hws_size = 0;
-  long long spin_cycles = 0;
+  long long spin_cycles = 0;   // budget of every bounded wait, in SM clock cycles
+  long long spin_default = 0;  // about 20 s at the maximum SM clock
   // phase timing (rfd_context_phase_times)
   int timing = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -730,6 +731,17 @@ struct rfd_context {
 namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// RFD_SPIN_CYCLES (a positive integer): the budget of every bounded wait, in SM clock
+// cycles, in place of the default of about 20 s.  A small budget makes waits run out (the
+// call then reports RFD_ERR_TIMEOUT), which is how the failure path is tested.
+long long env_spin_cycles(long long dflt) {
+  const char* e = getenv("RFD_SPIN_CYCLES");
+  if (!e || !*e) return dflt;
+  char* end = nullptr;
+  const long long v = strtoll(e, &end, 10);
+  return (end && *end == 0 && v > 0) ? v : dflt;
+}
 
 int ensure_device(rfd_context* ctx, size_t bytes) {
   if (bytes <= ctx->dws_size) return RFD_OK;
@@ -1390,7 +1402,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int flags[] = {mode, (int)on_device, (int)drop, ck, max_probes, o.stop_mode, o.reference_quirks,
                          o.dense, o.precision, o.bracket != nullptr, ctx->timing, ctx->prof,
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
-                         ctx->search_switch, ctx->search_window};
+                         ctx->search_switch, ctx->search_window, (int)(ctx->spin_cycles >> 32),
+                         (int)(ctx->spin_cycles & 0xffffffff)};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));
@@ -1622,8 +1635,9 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
   }
-  // wait budget: about 20 s at the maximum SM clock
-  c->spin_cycles = (long long)prop.clockRate * 1000LL * 20LL;
+  // wait budget: about 20 s at the maximum SM clock, or RFD_SPIN_CYCLES
+  c->spin_default = (long long)prop.clockRate * 1000LL * 20LL;
+  c->spin_cycles = env_spin_cycles(c->spin_default);
   if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     return fail(RFD_ERR_CUDA, "cudaStreamCreate");
@@ -1690,6 +1704,12 @@ int32_t rfd_fp64_peak(rfd_context* ctx, double* tflops) {
   if (e != cudaSuccess) return fail(RFD_ERR_CUDA, cudaGetErrorString(e));
   const double flops = 2.0 * 8.0 * (double)iters * (double)blocks * 256.0;
   *tflops = flops / (best * 1e-3) / 1e12;
+  return RFD_OK;
+}
+
+int32_t rfd_context_set_wait_budget(rfd_context* ctx, int64_t cycles) {
+  if (!ctx) return fail(RFD_ERR_ARG, "null context");
+  ctx->spin_cycles = cycles > 0 ? (long long)cycles : ctx->spin_default;
   return RFD_OK;
 }
 
@@ -2017,6 +2037,10 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   if (dims != 2 && dims != 3) return fail(RFD_ERR_ARG, "dims must be 2 or 3");
   if (n1 < 2 || n2 < 2) return fail(RFD_ERR_ARG, "decisions need curves of at least two points");
   if (!(radius >= 0.0)) return fail(RFD_ERR_ARG, "radius");
+  // the layout below is computed in size_t from these counts: bound them first (the
+  // engine's own per-curve limit), so no product can wrap past the array-size check
+  if (n1 > (1 << 30) || n2 > (1 << 30))
+    return fail(RFD_ERR_LIMIT, "rfd_decide_noalloc: curve longer than 2^30 points");
   int dev = 0;
   RFD_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(RFD_ERR_ARG, "device index above 63");
@@ -2102,7 +2126,7 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   wa.ticket = (unsigned*)(base + o_ticket);
   wa.error = (int*)(base + o_error);
   wa.active_pairs = (int*)(base + o_active);
-  wa.spin_cycles = nd.spin_cycles;
+  wa.spin_cycles = env_spin_cycles(nd.spin_cycles);
   wa.prof = nullptr;
   team_kernel<K_DEC><<<nd.team_grid, kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
   RFD_CUDA(cudaGetLastError());

@@ -8,8 +8,10 @@ This records, for fixed seeded inputs:
     FLT_EPSILON stop, midpoint) driving the oracle's DFD, VE-FD and decisions;
   - the endpoint bound as Point::dist_sqr computes it;
   - txtLoader2 / txtLoader3 on the edge-case files in tests/golden/txt/.
-The reference's GPU kernels are not run here.
+The reference's GPU kernels are not run here: this CPU has no GPU, and the harness replaces
+its GPU class with the oracle.
 
+    RFD_REFERENCE_DIR=<reference checkout> make -C oracle/refharness
     python tests/golden/make_reference_host_golden.py   # writes tests/golden/reference_host.json
 """
 import ctypes
