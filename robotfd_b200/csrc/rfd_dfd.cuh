@@ -77,8 +77,18 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   const int S = (R + H - 1) / H;
   const bool has_prod = s > 0;
   const bool has_cons = s + 1 < S;
-  const double* in_bnd = has_prod ? pd.bnd + (size_t)(s - 1) * pd.cstride : nullptr;
-  double* out_bnd = has_cons ? pd.bnd + (size_t)s * pd.cstride : nullptr;
+  // rows of the boundary ring, handed on column by column (see "Boundary ring" in
+  // rfd_device.cuh): this strip clears each input chunk once read, and writes an output column
+  // only where the row's previous reader has cleared it
+  const int nring = pd.ring;
+  const int slot_in = has_prod ? (s - 1) % nring : 0;
+  const int slot_out = has_cons ? s % nring : 0;
+  double* in_bnd = has_prod ? pd.bnd + (size_t)slot_in * pd.cstride : nullptr;
+  double* out_bnd = has_cons ? pd.bnd + (size_t)slot_out * pd.cstride : nullptr;
+  unsigned long long* in_slot = pd.slots + slot_in;
+  unsigned long long* out_slot = pd.slots + slot_out;
+  unsigned in_ok = 0, out_ok = 0;  // leading columns cleared for the input's / this strip's writer
+  constexpr int kPublish = 8;      // chunks between releases of the cleared count
 
   Waiter wt;
   wt.start(wa, st, s);
@@ -121,12 +131,20 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
 #pragma unroll
     for (int e = 0; e < DS; ++e) q[e] = __ldg(pd.Q + (size_t)j * DS + e);
   };
-  // the row above the strip at column 32c + lane (empty pattern while not yet written)
+  // the row above the strip at column 32c + lane (empty pattern while not yet written, or
+  // while the row may still hold its previous writer's words there)
   auto load_in = [&](int c) -> unsigned long long {
     const int col = (c << 5) + lane;
     if (!has_prod) return __double_as_longlong(col == 0 ? 0.0 : kFltMax);
     if ((c << 5) >= C || col >= C) return __double_as_longlong(kFltMax);
+    if (in_ok < (unsigned)min((c + 1) << 5, C)) return kBndEmpty;
     return ld_relaxed_u64(in_bnd + col);
+  };
+  // cleared count of a slot for writer `who` (acquire: the clearing stores are visible)
+  auto cleared = [&](unsigned long long* slot, int who, unsigned have) -> unsigned {
+    const unsigned long long w = bcast(lane == 0 ? ld_acquire(slot) : 0ull);
+    __syncwarp();  // every lane's later accesses of the row are ordered after the acquire
+    return (unsigned)(w >> 32) == (unsigned)who ? max(have, (unsigned)w) : have;
   };
   const bool store_out = has_cons && lane == 31;
 
@@ -200,7 +218,13 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   for (int c = 0; (c << 5) < nsteps; ++c) {
     // wait until every column of this chunk's input row has been written
     unsigned long long cur = nxt;
+    const bool reads = has_prod && (c << 5) < C;
+    const unsigned need_in = (unsigned)min((c + 1) << 5, C);
     for (int it = 0;; ++it) {
+      if (reads && in_ok < need_in) {
+        in_ok = cleared(in_slot, s - 1, in_ok);
+        if (in_ok >= need_in) cur = load_in(c);
+      }
       if (__all_sync(kFull, cur != kBndEmpty)) break;
       const int r = wt.check(it);
       if (r) {  // 1 cannot happen (the DFD has no dead strips); 2: error
@@ -210,6 +234,31 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
       if (cur == kBndEmpty) cur = load_in(c);
     }
     if (status) break;
+    if (reads) {
+      // read: the chunk's words go back to "not yet written" for the row's next writer
+      const int col = (c << 5) + lane;
+      if (col < C) st_relaxed_u64(reinterpret_cast<unsigned long long*>(in_bnd) + col, kBndEmpty);
+      if ((c & (kPublish - 1)) == kPublish - 1) {
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence();
+          st_release(in_slot, ((unsigned long long)(unsigned)(s - 1 + nring) << 32) | need_in);
+        }
+      }
+    }
+    if (has_cons) {
+      // this chunk's steps store the last row's columns below 32c + 32 - kOutLag
+      const unsigned need_out = (unsigned)min(max((c << 5) + 32 - kOutLag, 0), C);
+      for (int it = 0; out_ok < need_out; ++it) {
+        out_ok = cleared(out_slot, s, out_ok);
+        if (out_ok >= need_out) break;
+        if (wt.check(it)) {
+          status = 1;
+          break;
+        }
+      }
+      if (status) break;
+    }
     nxt = load_in(c + 1);  // in flight during this chunk
     fetch(c + 1, qn);
     if (c < kFirstChunks) steps(c, __longlong_as_double(cur), BoolC<true>{});
@@ -217,6 +266,14 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     __syncwarp();
     stage(c + 1, qn);
     __syncwarp();
+  }
+  if (status == 0 && has_prod) {
+    // every input word has been read and cleared: the whole row is the next writer's
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release(in_slot, ((unsigned long long)(unsigned)(s - 1 + nring) << 32) | kSlotAll);
+    }
   }
   if (holds_last) st->result = res;
   return status;

@@ -37,6 +37,14 @@ using namespace rfd;
 namespace {
 
 constexpr int kBlock = 128;
+
+// Boundary ring rows per pair.  Team strips: a decision's or VE-FD's band keeps only the
+// strips it passes through busy, and a strip claims a row only from a strip that ended, so
+// the ring holds the strips in flight with a wide margin (a band of w columns keeps about
+// w / 190 strips busy at once).  DFD strips hand rows on column by column and need only a few
+// strips' lag: kPublish chunks plus the publication's latency.
+constexpr int kTeamRingRows = 128;
+constexpr int kDfdRingRows = 32;
 thread_local std::string g_last_error;
 
 int fail(int code, const std::string& msg) {
@@ -329,11 +337,16 @@ __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_
     const PairDesc pd = pairs[p];
     const long long S = (pd.n1 + rows_per_strip - 1) / rows_per_strip;
     if (S < 2) continue;
+    const long long rows = min(S - 1, (long long)pd.ring);
     // cstride is a multiple of 32 doubles and bnd 256-byte aligned: 16-byte stores
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
-    const long long n = (S - 1) * pd.cstride / 2;
+    const long long n = rows * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
       b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
+    // ring row k is first written by strip k, every column of it cleared
+    if (blockIdx.x == 0)
+      for (int k = threadIdx.x; k < rows; k += blockDim.x)
+        pd.slots[k] = ((unsigned long long)k << 32) | kSlotAll;
   }
 }
 
@@ -366,10 +379,19 @@ __global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int 
     const PairDesc pd = pairs[p];
     const long long S = (pd.n1 - 1 + 31) / 32;
     if (S < 2) continue;
+    const long long rows = min(S - 1, (long long)pd.ring);
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
-    const long long n = (S - 1) * pd.cstride / 2;
+    const long long n = rows * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
       b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
+    // every ring row fresh for this phase's epoch, nothing written to it yet
+    if (blockIdx.x == 0) {
+      const unsigned E = st[p].epoch;
+      for (int k = threadIdx.x; k < rows; k += blockDim.x) {
+        pd.slots[k] = ((unsigned long long)E << 32) | kSlotFresh;
+        pd.slot_dirty[k] = make_int2(INT_MAX, -1);
+      }
+    }
   }
 }
 
@@ -553,14 +575,22 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
     }
     __syncthreads();
     if (KIND == K_DEC && sh->push) {
-      // the probe's written boundary words back to "not yet written", one strip per warp
+      // the ring rows' written words back to "not yet written" and every row fresh for the
+      // next probe's epoch (its tags are told apart by the epoch), one row per warp
       const long long C = pd.n2 - 1;
-      for (int r = warp; r < S - 1; r += kTeamThreads / 32) {
-        const int lo = pd.prog[r].wlo, hi = pd.prog[r].whi;
+      const unsigned E2 = *(volatile unsigned*)&st->epoch;
+      const int nrows = S > 1 ? min(pd.ring, S - 1) : 0;
+      for (int r = warp; r < nrows; r += kTeamThreads / 32) {
+        const int2 d = ld_volatile(pd.slot_dirty + r);
         double* row = pd.bnd + (size_t)r * pd.cstride;
-        const long long end = min((long long)(hi + 1) << 5, C);
-        for (long long w = ((long long)lo << 5) + lane; lo <= hi && w < end; w += 32)
+        const long long end = min((long long)(d.y + 1) << 5, C);
+        for (long long w = ((long long)d.x << 5) + lane; d.x <= d.y && w < end; w += 32)
           reinterpret_cast<unsigned long long*>(row)[w] = kBndEmpty;
+        __syncwarp();
+        if (lane == 0) {
+          st_volatile(pd.slot_dirty + r, make_int2(INT_MAX, -1));
+          pd.slots[r] = ((unsigned long long)E2 << 32) | kSlotFresh;
+        }
       }
       __threadfence();
       __syncthreads();
@@ -711,6 +741,10 @@ struct rfd_context {
   int dfd_grid_all[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // for rows 1, 2, 4, 8
   int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 1 row per lane
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
+  // rows of the boundary ring per pair (see "Boundary ring" in rfd_device.cuh): team strips
+  // (RFD_RING_ROWS) and DFD strips (RFD_DFD_RING_ROWS); at least 2
+  int ring_rows = kTeamRingRows;
+  int dfd_ring_rows = kDfdRingRows;
   void* dws = nullptr;
   size_t dws_size = 0;
   void* hws = nullptr;
@@ -731,6 +765,18 @@ struct rfd_context {
 namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+int ring_of(int64_t strips, int rows) {  // strips - 1 rows are handed over; at least 1
+  return (int)std::max<int64_t>(1, std::min<int64_t>(strips - 1, rows));
+}
+
+int env_rows(const char* name, int dflt) {
+  const char* e = getenv(name);
+  if (!e || !*e) return dflt;
+  char* end = nullptr;
+  const long v = strtol(e, &end, 10);
+  return (end && *end == 0 && v >= 2 && v <= (1 << 20)) ? (int)v : dflt;
+}
 
 // RFD_SPIN_CYCLES (a positive integer): the budget of every bounded wait, in SM clock
 // cycles, in place of the default of about 20 s.  A small budget makes waits run out (the
@@ -783,12 +829,32 @@ struct Layout {
   // device offsets
   size_t descs, tdescs, states, items, titems, counters, error, active, zero_begin, zero_end,
       total;
-  std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog;
+  std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog, slots, dirty;
+  std::vector<int> ring_d, ring_t, ring_c;  // ring rows: DFD, team strips, coarse DFD
   // host staging offsets
   size_t h_descs, h_tdescs, h_states, h_items, h_titems, h_misc, h_curves, h_total;
   std::vector<size_t> hP, hQ;
   int nitems, ntitems, nlaunch;
 };
+
+// Device workspace of one pair in a batch (an upper bound of what run_batch lays out for
+// it): curves, segment records, the boundary ring, tags, progress and slot words, items.
+double pair_workspace_bytes(const rfd_context* ctx, int64_t n1, int64_t n2, int d, int ck) {
+  const int64_t rows = std::min(n1, n2), cols = std::max(n1, n2);
+  const int64_t St = (std::max<int64_t>(rows - 1, 0) + 31) / 32;
+  const double rt = ctx->solo ? (double)std::max<int64_t>(St - 1, 1)
+                              : (double)ring_of(St, ctx->ring_rows);
+  const double rd = (double)ring_of((n1 + 31) / 32, ctx->dfd_ring_rows);
+  const double ring_words = std::max(rt * (double)(cols + 32), rd * (double)(n2 + 32));
+  double b = 8.0 * (double)d * (double)(n1 + n2)         // curves
+             + 16.0 * (double)rows + 64.0 * (double)cols  // segment records
+             + 8.0 * ring_words                           // boundary ring
+             + 4.0 * rt * (double)(cols / 32 + 64)        // tags
+             + 40.0 * (double)(St + 1) + 16.0 * (double)(n1 / 32 + rows / 32 + 2)  // progress, items
+             + 24.0 * (rt + rd) + 8192.0;                 // slot words, descriptors, state
+  if (ck) b += 8.0 * (double)(d + 1) * (double)(n1 + n2) / ck + 16384.0;
+  return b;
+}
 
 int check_pair(const double* c1, int64_t n1, const double* c2, int64_t n2, int32_t d) {
   if (!c1 || !c2) return fail(RFD_ERR_ARG, "null curve pointer");
@@ -903,6 +969,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   Layout L;
   L.P.resize(npairs); L.Q.resize(npairs); L.rowc.resize(npairs); L.colrec.resize(npairs);
   L.bnd.resize(npairs); L.tags.resize(npairs); L.prog.resize(npairs);
+  L.slots.resize(npairs); L.dirty.resize(npairs);
+  L.ring_d.resize(npairs); L.ring_t.resize(npairs); L.ring_c.resize(npairs);
   L.hP.resize(npairs); L.hQ.resize(npairs);
   const int ck = mode == MODE_DISTANCE ? o.coarse_ub : 0;  // coarse upper bound, every ck-th point
   auto coarse_n = [&](int64_t n) { return n < 2 ? n : (n - 2) / ck + 2; };  // anchors 0, ck, ..., n-1
@@ -958,11 +1026,21 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.counters = take(sizeof(unsigned) * (L.nlaunch + max_probes + 1));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
   L.error = take(sizeof(int));
-  for (int64_t p = 0; p < npairs; ++p) {  // progress words and tags: team strips only
-    const int64_t S = (trows(p) + 31) / 32;
+  for (int64_t p = 0; p < npairs; ++p) {
+    // ring rows: team strips of 32 segment rows; DFD strips of at least 32 point rows (the
+    // strip height the autotuner may pick); the coarse pair's DFD
+    const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
+    L.ring_t[p] = ctx->solo ? ring_of(St, INT32_MAX) : ring_of(St, ctx->ring_rows);
+    L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
+    L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
+                      ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
+    // progress words, tags (team strips) and slot words: cleared every call
     const int64_t tstride = align_up((size_t)((tcols(p) + 31) / 32), 32);
-    L.tags[p] = take(sizeof(unsigned) * (S > 1 ? S - 1 : 0) * tstride);
-    L.prog[p] = take(sizeof(Prog) * S);
+    L.tags[p] = take(sizeof(unsigned) * L.ring_t[p] * tstride);
+    L.prog[p] = take(sizeof(Prog) * std::max<int64_t>(St, (trows(p) + 31) / 32));
+    L.slots[p] = take(sizeof(unsigned long long) *
+                      std::max(L.ring_t[p], std::max(L.ring_d[p], L.ring_c[p])));
+    L.dirty[p] = take(sizeof(int2) * L.ring_t[p]);
   }
   L.zero_end = off;
   L.active = take(sizeof(int));
@@ -982,16 +1060,16 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
     const int d = dims[p];
-    const int64_t S = (n1 + 31) / 32;
     const int64_t cstride = align_up((size_t)n2, 32);
-    // segment records in the team strips' orientation; boundary rows for the DFD sweep
-    // (given orientation) and the team strips
-    const int64_t St = (trows(p) + 31) / 32;
+    // segment records in the team strips' orientation; the boundary ring, shared by the DFD
+    // sweep (given orientation), the coarse DFD and the team strips, which run one after another
     const int64_t tcstride = align_up((size_t)tcols(p), 32);
     L.rowc[p] = take(sizeof(double2) * std::max<int64_t>(trows(p) - 1, 1));
     L.colrec[p] = take(sizeof(double2) * (d == 2 ? 3 : 4) * std::max<int64_t>(tcols(p) - 1, 1));
-    L.bnd[p] = take(sizeof(double) * std::max((S > 1 ? S - 1 : 0) * cstride,
-                                              (St > 1 ? St - 1 : 0) * tcstride));
+    const int64_t ccstride = ck ? align_up((size_t)coarse_n(n2), 32) : 0;
+    L.bnd[p] = take(sizeof(double) * std::max(std::max((int64_t)L.ring_d[p] * cstride,
+                                                       (int64_t)L.ring_t[p] * tcstride),
+                                              (int64_t)L.ring_c[p] * ccstride));
     if (ck) {
       // anchors and their inflations; a pair with a one-point curve keeps every point, with
       // inflation 0 (its DFD is its exact, closed-form answer)
@@ -1035,7 +1113,6 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   for (int64_t p = 0; p < npairs; ++p) {
     const int64_t n1 = n1s[p], n2 = n2s[p];
     const int d = dims[p];
-    const int64_t S = (n1 + 31) / 32;
     PairDesc& D = hd[p];
     memset(&D, 0, sizeof(D));
     if (on_device && !dcompact) {
@@ -1055,14 +1132,17 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     D.bnd = (double*)(dbase + L.bnd[p]);
     D.tags = (unsigned*)(dbase + L.tags[p]);
     D.prog = (Prog*)(dbase + L.prog[p]);
+    D.slots = (unsigned long long*)(dbase + L.slots[p]);
+    D.slot_dirty = (int2*)(dbase + L.dirty[p]);
+    D.ring = L.ring_d[p];
     D.n1 = (int)n1;
     D.n2 = (int)n2;
     D.d = d;
     D.cstride = (long long)align_up((size_t)n2, 32);
     D.tstride = (long long)align_up((size_t)((n2 + 31) / 32), 32);
-    (void)S;
     PairDesc& Dt = ((PairDesc*)(hbase + L.h_tdescs))[p];
     Dt = D;
+    Dt.ring = L.ring_t[p];
     if (trv[p]) {
       Dt.P = D.Q;
       Dt.Q = D.P;
@@ -1084,6 +1164,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         Dc.n1 = (int)coarse_n(n1);
         Dc.n2 = (int)coarse_n(n2);
         Dc.cstride = (long long)align_up((size_t)Dc.n2, 32);
+        Dc.ring = L.ring_c[p];
       }
     }
     PairState& s = hs[p];
@@ -1634,6 +1715,8 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     }
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
+    c->ring_rows = env_rows("RFD_RING_ROWS", kTeamRingRows);
+    c->dfd_ring_rows = env_rows("RFD_DFD_RING_ROWS", kDfdRingRows);
   }
   // wait budget: about 20 s at the maximum SM clock, or RFD_SPIN_CYCLES
   c->spin_default = (long long)prop.clockRate * 1000LL * 20LL;
@@ -1731,7 +1814,50 @@ int32_t rfd_distance_batch(rfd_context* ctx, int64_t npairs, const double* const
                            const int32_t* dims, const rfd_options* opt, rfd_result* out) {
   if (!ctx) return fail(RFD_ERR_ARG, "null context");
   RFD_CUDA(cudaSetDevice(ctx->device));
-  return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+  if (npairs <= 1 || !c1s || !n1s || !c2s || !n2s || !dims || !out)
+    return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+  // Pairs go in chunks whose device workspace stays within the budget: RFD_BATCH_BUDGET
+  // bytes, else 3/4 of the device memory this context may use (its workspace and what is
+  // free).  A call that fits runs whole (and may be a CUDA graph); chunks run one after
+  // another without one.  Results do not depend on the chunking.
+  double budget = 0.0;
+  if (const char* e = getenv("RFD_BATCH_BUDGET")) budget = atof(e);
+  if (!(budget > 0.0)) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    budget = 0.75 * ((double)fr + (double)ctx->dws_size);
+  }
+  const int ck = opt ? opt->coarse_ub : 0;
+  std::vector<double> bytes((size_t)npairs);
+  double total = 0.0;
+  for (int64_t p = 0; p < npairs; ++p) {
+    if (n1s[p] < 1 || n2s[p] < 1 || (dims[p] != 2 && dims[p] != 3))
+      return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+    bytes[p] = pair_workspace_bytes(ctx, n1s[p], n2s[p], dims[p], ck);
+    total += bytes[p];
+  }
+  if (total <= budget)
+    return run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, opt, out, MODE_DISTANCE, 0.0);
+  rfd_options o;
+  rfd_options_init(&o, 0);
+  if (opt) o = *opt;
+  o.graph = 0;
+  int64_t p0 = 0;
+  while (p0 < npairs) {
+    int64_t p1 = p0 + 1;
+    double acc = bytes[p0];
+    while (p1 < npairs && acc + bytes[p1] <= budget) acc += bytes[p1++];
+    rfd_options oc = o;
+    if (o.bracket) oc.bracket = o.bracket + 2 * p0;  // per-pair bracket: this chunk's slice
+    const int rc = run_batch(ctx, p1 - p0, c1s + p0, n1s + p0, c2s + p0, n2s + p0, dims + p0, &oc,
+                             out + p0, MODE_DISTANCE, 0.0);
+    if (rc) return rc;
+    p0 = p1;
+  }
+  return RFD_OK;
 }
 
 // Autotuner of the DFD sweep's tile shape: rows per lane (the strip height, 32 x 1, 2, 4 or 8)
@@ -1801,8 +1927,8 @@ int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* con
   if (ncurves > (1 << 20)) return fail(RFD_ERR_LIMIT, "more than 2^20 curves");
   if (opt && opt->bracket) return fail(RFD_ERR_ARG, "distance_matrix takes no per-pair bracket");
   RFD_CUDA(cudaSetDevice(ctx->device));
-  // pairs (i, j), i < j, go to the batch engine in chunks whose strip boundary rows (n1 n2 / 4
-  // bytes a pair, the bulk of the workspace) stay within the budget
+  // pairs (i, j), i < j, go to the batch engine in chunks whose workspace (the boundary ring,
+  // O(ring rows x columns) a pair, is the bulk of it) stays within the budget
   const double budget = budget_bytes > 0.0 ? budget_bytes : 8e9;
   const int64_t N = ncurves;
   std::vector<const double*> c1, c2;
@@ -1829,7 +1955,8 @@ int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* con
   for (int64_t i = 0; i < N; ++i)
     for (int64_t j = i + 1; j < N; ++j) {
       if (dims[i] != dims[j]) return fail(RFD_ERR_ARG, "curves of a pair differ in dimension");
-      const double bytes = (double)ns[i] * (double)ns[j] / 4.0 + 256.0 * (double)(ns[i] + ns[j]);
+      const double bytes =
+          pair_workspace_bytes(ctx, ns[i], ns[j], dims[i], opt ? opt->coarse_ub : 0);
       if (acc + bytes > budget && !where.empty()) {
         const int rc = flush();
         if (rc) return rc;
@@ -1994,6 +2121,7 @@ int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32
 namespace {
 
 constexpr size_t kNoAllocBytes = (size_t)64 << 20;  // 64 MiB
+constexpr int kNoAllocRing = 32;  // boundary ring rows
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 struct NoAllocDevice {
@@ -2067,8 +2195,10 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
     }
   }
   const NoAllocDevice nd = g_noalloc[dev];
-  // layout inside the array (same records as the allocating path)
-  const int64_t S = (n1 + 31) / 32;
+  // layout inside the array (same records as the allocating path; the strips hand rows
+  // over through a ring of kNoAllocRing rows, so the array holds pairs of any row count)
+  const int64_t S = (n1 - 1 + 31) / 32;  // 32-row strips over the n1 - 1 segment rows
+  const int ring = ring_of(S, kNoAllocRing);
   const int64_t cstride = (int64_t)align_up((size_t)n2, 32);
   const int64_t tstride = (int64_t)align_up((size_t)((n2 + 31) / 32), 32);
   size_t off = 0;
@@ -2079,13 +2209,15 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   const size_t o_zero = off;
   const size_t o_ticket = take(sizeof(unsigned));
   const size_t o_error = take(sizeof(int));
-  const size_t o_tags = take(sizeof(unsigned) * (size_t)(S - 1) * tstride);
+  const size_t o_tags = take(sizeof(unsigned) * (size_t)ring * tstride);
   const size_t o_prog = take(sizeof(Prog) * S);
+  const size_t o_slots = take(sizeof(unsigned long long) * ring);
+  const size_t o_dirty = take(sizeof(int2) * ring);
   const size_t zero_end = off;
   const size_t o_active = take(sizeof(int));
   const size_t o_rowc = take(sizeof(double2) * (size_t)(n1 - 1));
   const size_t o_colrec = take(sizeof(double2) * (dims == 2 ? 3 : 4) * (size_t)(n2 - 1));
-  const size_t o_bnd = take(sizeof(double) * (size_t)(S - 1) * cstride);
+  const size_t o_bnd = take(sizeof(double) * (size_t)ring * cstride);
   if (off > kNoAllocBytes)
     return fail(RFD_ERR_LIMIT, "rfd_decide_noalloc: the pair needs " + std::to_string(off) +
                                    " bytes of scratch, the fixed array holds " +
@@ -2100,6 +2232,9 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   d.bnd = (double*)(base + o_bnd);
   d.tags = (unsigned*)(base + o_tags);
   d.prog = (Prog*)(base + o_prog);
+  d.slots = (unsigned long long*)(base + o_slots);
+  d.slot_dirty = (int2*)(base + o_dirty);
+  d.ring = ring;
   d.n1 = (int)n1;
   d.n2 = (int)n2;
   d.d = dims;
