@@ -140,11 +140,16 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     if (in_ok < (unsigned)min((c + 1) << 5, C)) return kBndEmpty;
     return ld_relaxed_u64(in_bnd + col);
   };
-  // cleared count of a slot for writer `who` (acquire: the clearing stores are visible)
+  // Cleared count of a slot for writer `who` (acquire: the clearing stores are visible).
+  // The word names a later writer only once the row's reader of `who`'s round has seen every
+  // column cleared for `who` (that reader publishes nothing before), so a later name means
+  // every column.
   auto cleared = [&](unsigned long long* slot, int who, unsigned have) -> unsigned {
     const unsigned long long w = bcast(lane == 0 ? ld_acquire(slot) : 0ull);
     __syncwarp();  // every lane's later accesses of the row are ordered after the acquire
-    return (unsigned)(w >> 32) == (unsigned)who ? max(have, (unsigned)w) : have;
+    const int id = (int)(unsigned)(w >> 32);
+    if (id == who) return max(have, (unsigned)w);
+    return id > who ? kSlotAll : have;
   };
   const bool store_out = has_cons && lane == 31;
 
@@ -235,10 +240,13 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     }
     if (status) break;
     if (reads) {
-      // read: the chunk's words go back to "not yet written" for the row's next writer
+      // read: the chunk's words go back to "not yet written" for the row's next writer.  The
+      // count is published only once the row's previous reader has published all of it
+      // (in_ok == kSlotAll): the slot word then passes from that reader to this one, and a
+      // later publication of that reader cannot overwrite this one's.
       const int col = (c << 5) + lane;
       if (col < C) st_relaxed_u64(reinterpret_cast<unsigned long long*>(in_bnd) + col, kBndEmpty);
-      if ((c & (kPublish - 1)) == kPublish - 1) {
+      if ((c & (kPublish - 1)) == kPublish - 1 && in_ok == kSlotAll) {
         __syncwarp();
         if (lane == 0) {
           __threadfence();
@@ -268,7 +276,17 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     __syncwarp();
   }
   if (status == 0 && has_prod) {
-    // every input word has been read and cleared: the whole row is the next writer's
+    // every input word has been read and cleared: the whole row is the next writer's, once
+    // the previous reader's last publication is in (see above)
+    for (int it = 0; in_ok != kSlotAll; ++it) {
+      in_ok = cleared(in_slot, s - 1, in_ok);
+      if (in_ok != kSlotAll && wt.check(it)) {
+        status = 1;
+        break;
+      }
+    }
+  }
+  if (status == 0 && has_prod) {
     __syncwarp();
     if (lane == 0) {
       __threadfence();
