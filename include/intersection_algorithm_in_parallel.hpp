@@ -2,7 +2,8 @@
 // include/intersection_algorithm_in_parallel.hpp:11-61).  It keeps the reference's
 // methods; each call runs on librfd.so (include/rfd.h):
 //   Bound_call_gpu(&ub, &lb)            -> rfd_bounds   (lb in: endpoint bound, out: VE-FD)
-//   intersection_interval_call_gpu(r)   -> rfd_decide
+//   intersection_interval_call_gpu(r)   -> rfd_decide_formula (the constructor's path choice:
+//                                          *forceOversize in/out, as in the reference)
 // The device buffers live in the library's context, so data_move and free_memory only
 // manage the host copies.
 #pragma once

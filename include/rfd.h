@@ -42,6 +42,19 @@ enum rfd_stop {
 
 enum rfd_memory { RFD_MEM_HOST = 0, RFD_MEM_DEVICE = 1 };
 
+/* Free intervals of the decision.  The reference has two decision paths and picks one per
+   solve by free device memory (src/intersection_algorithm_in_parallel.cu:87-97): the
+   materialised one when 4 (n1-1)(n1+n2-4) doubles of intervals fit, else the fused
+   ("oversize") kernel.  They round C of the free-interval quadratic differently
+   (interval_calculation .cu:742 forms (sum mi^2) - r^2; reachable .cu:1177-1186 starts the sum
+   at -r^2), so a decision within a few ulps of the distance can differ between them. */
+enum rfd_formula {
+  RFD_FORMULA_FUSED = 0,         /* reachable<d> (.cu:960-1256), forceOversize's path */
+  RFD_FORMULA_MATERIALISED = 1,  /* interval_calculation<d> + reachability (.cu:673-958) */
+  RFD_FORMULA_REFERENCE = 2      /* per pair, the reference's choice on this device's free
+                                    memory at call time (its rule, .cu:92) */
+};
+
 enum rfd_precision {
   RFD_PREC_FP64 = 0,       /* every interval in FP64 */
   RFD_PREC_FP32_FILTER = 1 /* FP32 classification with a proven margin, FP64 recheck */
@@ -100,6 +113,8 @@ typedef struct rfd_options {
                                as one CUDA graph and keep it in the context; a later call with
                                the same layout (pair sizes, options, workspace, stream) replays
                                it instead of issuing each launch.  Results are identical. */
+  int32_t formula;          /* enum rfd_formula, default RFD_FORMULA_FUSED.  The FP32 filter
+                               certifies the fused intervals only: it needs RFD_FORMULA_FUSED. */
 } rfd_options;
 
 typedef struct rfd_result {
@@ -204,6 +219,14 @@ int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double*
    (include/intersection_algorithm_in_parallel.hpp:19, src/intersection_algorithm_in_parallel.cu:1398). */
 int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
                    int32_t dims, double radius, int32_t dense, int32_t* reachable, double* right_ub);
+
+/* rfd_decide with the free intervals of either reference decision path (enum rfd_formula;
+   RFD_FORMULA_REFERENCE picks by free device memory as the reference's constructor does,
+   src/intersection_algorithm_in_parallel.cu:87-97).  rfd_decide is this with
+   RFD_FORMULA_FUSED. */
+int32_t rfd_decide_formula(rfd_context* ctx, const double* c1, int64_t n1, const double* c2,
+                           int64_t n2, int32_t dims, double radius, int32_t dense, int32_t formula,
+                           int32_t* reachable, double* right_ub);
 
 /* One reachability decision that allocates nothing (no counterpart in the reference).
    For callers that cannot allocate device memory once they run: a robot's control loop

@@ -1,7 +1,10 @@
 // Public entry point (drop-in for the reference's include/wrapper.hpp:1-4): the continuous
 // Frechet distance of two curves, stop rule ub - lb <= FLT_EPSILON as in
-// src/compute_distance_wrapper.cpp:6.  forceOversize is accepted for source compatibility;
-// this engine always runs the O(n+m)-memory fused decision.
+// src/compute_distance_wrapper.cpp:6.  forceOversize chooses between the reference's two
+// decision paths as the reference does: forced, or when the reference's materialised interval
+// arrays would not fit in free device memory, the fused kernel's free intervals; otherwise the
+// materialised path's (they differ in one rounding, rfd.h enum rfd_formula).  The engine's
+// decision memory is O(ring rows x (n1 + n2)) either way.
 #pragma once
 
 #include "curve.hpp"

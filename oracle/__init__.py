@@ -48,6 +48,11 @@ def lib():
         L.rfd_oracle_distance.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, _dp, _ip, _dp, _ip]
+        L.rfd_oracle_decide_formula.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_int, ctypes.c_int, _dp]
+        L.rfd_oracle_distance_formula.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, _dp, _ip, _dp, _ip]
         L.rfd_oracle_search.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_int, _dp, _ip]
@@ -57,6 +62,9 @@ def lib():
         L.rfd_verify_free_bounds.argtypes = [_dp, _dp, _dp, ctypes.c_double, ctypes.c_int, _dp]
         L.rfd_oracle_free_intervals.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, ctypes.c_double,
                                                 ctypes.c_int, _dp, _dp]
+        L.rfd_oracle_free_intervals_formula.argtypes = [i64, _dp, _dp, _dp, _dp, _dp,
+                                                        ctypes.c_double, ctypes.c_int,
+                                                        ctypes.c_int, _dp, _dp]
         L.rfd_oracle_gen_pair.argtypes = [ctypes.c_int, ctypes.c_int, i64, i64, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _dp,
                                           ctypes.POINTER(i64), _dp, ctypes.POINTER(i64)]
@@ -107,12 +115,13 @@ def vefd_sq(P, Q, lb, threads=1):
     return out.value
 
 
-def decide(P, Q, radius, threads=1):
-    """Returns (reachable, propagated right UB of the last cell)."""
+def decide(P, Q, radius, threads=1, formula=0):
+    """Returns (reachable, propagated right UB of the last cell).  formula 0: the reference's
+    fused decision kernel's free intervals, 1: its materialised path's (mm - r^2)."""
     P, Q = _arr(P), _arr(Q)
     out = ctypes.c_double()
-    rc = lib().rfd_oracle_decide(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], radius, threads,
-                                 ctypes.byref(out))
+    rc = lib().rfd_oracle_decide_formula(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], radius,
+                                         formula, threads, ctypes.byref(out))
     if rc:
         raise RuntimeError(f"oracle decide failed ({rc})")
     return out.value == 1.0, out.value
@@ -122,8 +131,9 @@ FLT_EPSILON = float(np.finfo(np.float32).eps)
 REL_TOL = 2.0 ** -33
 
 
-def distance(P, Q, stop_mode=0, tol=None, quirks=True, max_probes=200, threads=1):
-    """Full search.  stop_mode 0 is the reference rule (ub-lb > FLT_EPSILON)."""
+def distance(P, Q, stop_mode=0, tol=None, quirks=True, max_probes=200, threads=1, formula=0):
+    """Full search.  stop_mode 0 is the reference rule (ub-lb > FLT_EPSILON); formula as in
+    decide()."""
     P, Q = _arr(P), _arr(Q)
     if tol is None:
         tol = FLT_EPSILON if stop_mode == 0 else REL_TOL
@@ -131,9 +141,10 @@ def distance(P, Q, stop_mode=0, tol=None, quirks=True, max_probes=200, threads=1
     probes = ctypes.c_int()
     log_eps = (ctypes.c_double * max(1, max_probes))()
     log_dec = (ctypes.c_int * max(1, max_probes))()
-    rc = lib().rfd_oracle_distance(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], stop_mode, tol,
-                                   int(bool(quirks)), max_probes, threads, out,
-                                   ctypes.byref(probes), log_eps, log_dec)
+    rc = lib().rfd_oracle_distance_formula(_ptr(P), len(P), _ptr(Q), len(Q), P.shape[1],
+                                           stop_mode, tol, int(bool(quirks)), max_probes,
+                                           threads, formula, out, ctypes.byref(probes), log_eps,
+                                           log_dec)
     if rc:
         raise RuntimeError(f"oracle distance failed ({rc})")
     n = probes.value
@@ -159,15 +170,17 @@ def search(P, Q, lb, ub, stop_mode=0, tol=None, max_probes=200, threads=1):
     return out[0], out[1], out[2], probes.value
 
 
-def free_intervals(x, a, b, A, r2):
-    """FP64 free intervals of the edges a_e -> b_e around x_e (arrays [n][d]; A [n])."""
+def free_intervals(x, a, b, A, r2, formula=0):
+    """FP64 free intervals of the edges a_e -> b_e around x_e (arrays [n][d]; A [n]); formula
+    as in decide()."""
     x, a, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, a, b))
     A = np.ascontiguousarray(A, dtype=np.float64)
     inv2A = 0.5 / A
     n, d = x.shape
     lo, hi = np.empty(n), np.empty(n)
-    rc = lib().rfd_oracle_free_intervals(n, _ptr(x), _ptr(a), _ptr(b), _ptr(A), _ptr(inv2A),
-                                         float(r2), d, _ptr(lo), _ptr(hi))
+    rc = lib().rfd_oracle_free_intervals_formula(n, _ptr(x), _ptr(a), _ptr(b), _ptr(A),
+                                                 _ptr(inv2A), float(r2), d, int(formula),
+                                                 _ptr(lo), _ptr(hi))
     if rc:
         raise RuntimeError("oracle free_intervals failed")
     return lo, hi

@@ -67,6 +67,7 @@ typedef struct {
   double *bot;           /* [R] running value along each row */
   double last_ub;        /* decision: propagated right UB of the last cell */
   double last_val;       /* DP: value at the last cell */
+  int mat;               /* decision: the materialised path's rounding of C (see free_interval) */
 } ora_t;
 
 /* |a-b|^2 by an fma chain from 0.0 (DFD .cu:615-619). */
@@ -111,16 +112,19 @@ static inline double pt_seg_sq(const double* x, const double* a, const double* b
 }
 
 /* Free interval of segment a -> b inside the ball of radius^2 r2 around x (.cu:1175-1199):
-   di = b - a, mi = a - x, B = 2*sum(mi*di), Cc = -r2 + sum(mi^2), disc = B^2 - 4*A*Cc. */
+   di = b - a, mi = a - x, B = 2*sum(mi*di), Cc = -r2 + sum(mi^2), disc = B^2 - 4*A*Cc.
+   mat: the materialised path's C (interval_calculation, .cu:730-742 and :765-776): the sum
+   of mi^2 from 0, then minus r2 (mm - radius2), one rounding more than the fused chain. */
 static inline void free_interval(const double* x, const double* a, const double* b, double A,
-                                 double inv2A, double r2, int d, double* lo, double* hi) {
-  double B = 0.0, Cc = -r2;
+                                 double inv2A, double r2, int d, int mat, double* lo, double* hi) {
+  double B = 0.0, Cc = mat ? 0.0 : -r2;
   for (int k = 0; k < d; ++k) {
     double di = b[k] - a[k];
     double mi = a[k] - x[k];
     B = fma(mi, di, B);
     Cc = fma(mi, mi, Cc);
   }
+  if (mat) Cc = Cc - r2;
   B = B * 2.0;
   double disc = fma(B, B, -((4.0 * A) * Cc));
   *lo = -1.0;
@@ -186,9 +190,9 @@ static void tile(ora_t* o, int64_t i0, int64_t i1, int64_t j0, int64_t j1) {
         double leftLB = o->down[j];
         double rLB, rUB, tLB, tUB;
         /* right edge: ball around p_{i+1}, segment q_j -> q_{j+1} */
-        free_interval(pa2, qb1, qb2, o->colA[j], o->colInv[j], o->r2, d, &rLB, &rUB);
+        free_interval(pa2, qb1, qb2, o->colA[j], o->colInv[j], o->r2, d, o->mat, &rLB, &rUB);
         /* top edge: ball around q_{j+1}, segment p_i -> p_{i+1} */
-        free_interval(qb2, pa1, pa2, Aa, inv2Aa, o->r2, d, &tLB, &tUB);
+        free_interval(qb2, pa1, pa2, Aa, inv2Aa, o->r2, d, o->mat, &tLB, &tUB);
         if (b < 0.0) {
           int invalid = (leftLB > rUB) || (leftLB < 0.0);
           double m = cmax(rLB, leftLB);
@@ -251,12 +255,12 @@ static int prep_segments(const double* X, int64_t n, int d, double** A, double**
   return 0;
 }
 
-static int run(int kind, const double* P, int64_t n1, const double* Q, int64_t n2, int d,
-               double r2, double seed, int threads, double* out_ub, double* out_val) {
+static int run_mat(int kind, const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+                   double r2, double seed, int mat, int threads, double* out_ub, double* out_val) {
   ora_t o;
   memset(&o, 0, sizeof(o));
   o.kind = kind;
-  o.d = d;
+  o.mat = mat;  o.d = d;
   o.P = P;
   o.Q = Q;
   o.r2 = r2;
@@ -291,6 +295,12 @@ static int run(int kind, const double* P, int64_t n1, const double* Q, int64_t n
   return 0;
 }
 
+
+static int run(int kind, const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+               double r2, double seed, int threads, double* out_ub, double* out_val) {
+  return run_mat(kind, P, n1, Q, n2, d, r2, seed, 0, threads, out_ub, out_val);
+}
+
 /* ------------------------------------------------------------------ exports */
 
 double rfd_oracle_endpoint(const double* P, int64_t n1, const double* Q, int64_t n2, int d) {
@@ -319,12 +329,36 @@ int rfd_oracle_decide(const double* P, int64_t n1, const double* Q, int64_t n2, 
   return run(K_DEC, P, n1, Q, n2, d, r2, 0.0, threads, right_ub, NULL);
 }
 
+/* The same with the free intervals of either reference path: formula 0 the fused kernel
+   reachable<d> (.cu:1173-1244, taken with forceOversize or when memory is short), 1 the
+   materialised interval_calculation<d> (.cu:725-789), whose propagation (reachability,
+   .cu:907-934) is the fused one. */
+int rfd_oracle_decide_formula(const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+                              double radius, int formula, int threads, double* right_ub) {
+  double r2 = radius * radius;
+  return run_mat(K_DEC, P, n1, Q, n2, d, r2, 0.0, formula == 1, threads, right_ub, NULL);
+}
+
 /* Full search.  stop_mode 0: while (ub-lb > tol) (reference); 1: while (ub-lb > tol*ub).
    quirks: skip VE-FD when (int)(n1*n2) <= 10000.  Optional logs of every probe. */
+int rfd_oracle_distance_formula(const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+                                int stop_mode, double tol, int quirks, int max_probes, int threads,
+                                int formula, double* out, int* out_probes, double* log_eps,
+                                int* log_dec);
+
 int rfd_oracle_distance(const double* P, int64_t n1, const double* Q, int64_t n2, int d,
                         int stop_mode, double tol, int quirks, int max_probes, int threads,
                         double* out /* [distance, dfd, vefd, endpoint, lb, ub] */,
                         int* out_probes, double* log_eps, int* log_dec) {
+  return rfd_oracle_distance_formula(P, n1, Q, n2, d, stop_mode, tol, quirks, max_probes, threads,
+                                     0, out, out_probes, log_eps, log_dec);
+}
+
+/* Full search with the decisions of either reference path (rfd_oracle_decide_formula). */
+int rfd_oracle_distance_formula(const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+                                int stop_mode, double tol, int quirks, int max_probes, int threads,
+                                int formula, double* out, int* out_probes, double* log_eps,
+                                int* log_dec) {
   double endpoint = rfd_oracle_endpoint(P, n1, Q, n2, d);
   double dsq, vsq, ub, lb = endpoint;
   if (n1 < 2 || n2 < 2) return -1;
@@ -344,7 +378,7 @@ int rfd_oracle_distance(const double* P, int64_t n1, const double* Q, int64_t n2
     double split = (ub + lb) / 2.0;
     if (!(split > lb && split < ub)) break;
     double rub;
-    if (rfd_oracle_decide(P, n1, Q, n2, d, split, threads, &rub)) return -2;
+    if (rfd_oracle_decide_formula(P, n1, Q, n2, d, split, formula, threads, &rub)) return -2;
     int reach = rub == 1.0;
     if (log_eps) log_eps[probes] = split;
     if (log_dec) log_dec[probes] = reach;
@@ -389,13 +423,20 @@ int rfd_oracle_search(const double* P, int64_t n1, const double* Q, int64_t n2, 
 
 /* Free intervals of n edges (test entry): edge e is the segment a_e -> b_e against the ball
    of radius^2 r2 around x_e, with A_e = |b_e - a_e|^2 and inv2A_e = 0.5 / A_e as given. */
+int rfd_oracle_free_intervals_formula(int64_t n, const double* x, const double* a,
+                                      const double* b, const double* A, const double* inv2A,
+                                      double r2, int d, int formula, double* lo, double* hi) {
+  if (n < 0 || (d != 2 && d != 3)) return 1;
+  for (int64_t e = 0; e < n; ++e)
+    free_interval(x + e * d, a + e * d, b + e * d, A[e], inv2A[e], r2, d, formula == 1, lo + e,
+                  hi + e);
+  return 0;
+}
+
 int rfd_oracle_free_intervals(int64_t n, const double* x, const double* a, const double* b,
                               const double* A, const double* inv2A, double r2, int d, double* lo,
                               double* hi) {
-  if (n < 0 || (d != 2 && d != 3)) return 1;
-  for (int64_t e = 0; e < n; ++e)
-    free_interval(x + e * d, a + e * d, b + e * d, A[e], inv2A[e], r2, d, lo + e, hi + e);
-  return 0;
+  return rfd_oracle_free_intervals_formula(n, x, a, b, A, inv2A, r2, d, 0, lo, hi);
 }
 
 int rfd_oracle_max_threads(void) {

@@ -32,6 +32,9 @@ RFD_MEM_HOST = 0
 RFD_MEM_DEVICE = 1
 RFD_PREC_FP64 = 0
 RFD_PREC_FP32_FILTER = 1
+RFD_FORMULA_FUSED = 0
+RFD_FORMULA_MATERIALISED = 1
+RFD_FORMULA_REFERENCE = 2
 
 FLAG_VEFD_SKIPPED = 1
 FLAG_LB_GT_UB = 2
@@ -52,7 +55,8 @@ EXPORTS = (
     "rfd_context_create", "rfd_context_destroy", "rfd_context_set_stream",
     "rfd_context_set_wait_budget",
     "rfd_context_phase_times", "rfd_fp64_peak", "rfd_distance",
-    "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_load_txt", "rfd_free",
+    "rfd_distance_batch", "rfd_bounds", "rfd_decide", "rfd_decide_formula", "rfd_load_txt",
+    "rfd_free",
     "rfd_gen_pair", "rfd_gen_batch_spec", "rfd_search_step", "rfd_decide_noalloc",
     "rfd_model_num_params", "rfd_model_create", "rfd_model_destroy", "rfd_model_set_params",
     "rfd_model_get_params", "rfd_model_forward", "rfd_model_gradients", "rfd_model_train_step",
@@ -81,6 +85,7 @@ class Options(ctypes.Structure):
         ("coarse_ub", ctypes.c_int32),
         ("drop_repeats", ctypes.c_int32),
         ("graph", ctypes.c_int32),
+        ("formula", ctypes.c_int32),
     ]
 
 
@@ -152,6 +157,8 @@ def lib():
     L.rfd_bounds.restype = i32
     L.rfd_decide.argtypes = [vp, vp, i64, vp, i64, i32, dbl, i32, _i32p, _dp]
     L.rfd_decide.restype = i32
+    L.rfd_decide_formula.argtypes = [vp, vp, i64, vp, i64, i32, dbl, i32, i32, _i32p, _dp]
+    L.rfd_decide_formula.restype = i32
     L.rfd_load_txt.argtypes = [ctypes.c_char_p, i32, i32, i32, ctypes.POINTER(_dp), _i64p]
     L.rfd_load_txt.restype = i32
     L.rfd_load_txt_fast.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, ctypes.POINTER(_dp), _i64p]
@@ -225,7 +232,8 @@ def _curve(c):
 
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
-            precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False, graph=False):
+            precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False, graph=False,
+            formula=0):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -241,6 +249,7 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
     o.coarse_ub = int(coarse_ub)
     o.drop_repeats = int(bool(drop_repeats))
     o.graph = int(bool(graph))
+    o.formula = int(formula)
     return o
 
 
@@ -329,13 +338,13 @@ class Context:
                                 ctypes.byref(vefd)))
         return dfd.value, vefd.value
 
-    def decide(self, P, Q, radius, dense=False):
+    def decide(self, P, Q, radius, dense=False, formula=RFD_FORMULA_FUSED):
         P, Q = _curve(P), _curve(Q)
         reach = ctypes.c_int32()
         rub = ctypes.c_double()
-        _check(lib().rfd_decide(self._h, P.ctypes.data, len(P), Q.ctypes.data, len(Q), P.shape[1],
-                                float(radius), int(bool(dense)), ctypes.byref(reach),
-                                ctypes.byref(rub)))
+        _check(lib().rfd_decide_formula(self._h, P.ctypes.data, len(P), Q.ctypes.data, len(Q),
+                                        P.shape[1], float(radius), int(bool(dense)), int(formula),
+                                        ctypes.byref(reach), ctypes.byref(rub)))
         return bool(reach.value), rub.value
 
     # ---- batch
@@ -431,9 +440,11 @@ def default_context():
 
 def compute_distance_parallel(curve1, curve2, force_oversize=False):
     """Mirror of the reference's compute_distance_parallel (include/wrapper.hpp:4): stop rule
-    ub - lb <= FLT_EPSILON, VE-FD launch rule of the reference, result (lb + ub) / 2."""
-    del force_oversize  # accepted for compatibility; the fused O(n+m) decision always runs
-    return default_context().distance(curve1, curve2)["distance"]
+    ub - lb <= FLT_EPSILON, VE-FD launch rule of the reference, result (lb + ub) / 2, and the
+    reference's choice of decision path: the fused kernel's free intervals when forced, else by
+    free device memory (RFD_FORMULA_REFERENCE)."""
+    formula = RFD_FORMULA_FUSED if force_oversize else RFD_FORMULA_REFERENCE
+    return default_context().distance(curve1, curve2, formula=formula)["distance"]
 
 
 def _load(path, dims, start, limit, threads=None):

@@ -108,6 +108,7 @@ struct PairState {
   int use_model;
   int filter;  // 1: decision intervals through the FP32 filter (RFD_PREC_FP32_FILTER)
   int coarse;  // 1: the DFD phase computes the coarse upper bound (rfd_options.coarse_ub)
+  int formula;  // decision intervals: 0 the fused path's, 1 the materialised path's (rfd.h)
   int pushed;      // continuous search: queue entries of the running probe so far (<= strips)
   int next_strip;  // continuous search: strips of the running probe taken so far
 };
@@ -222,18 +223,21 @@ __device__ __forceinline__ double pt_seg_sq(const double* x, const double* a, co
 }
 
 // Free interval on segment a -> a + di inside the ball of radius^2 r2 around x
-// (reference .cu:1175-1230).  Empty: (-1, -2).
+// (reference .cu:1175-1230).  Empty: (-1, -2).  mat: the reference's materialised path
+// (interval_calculation, .cu:730-742 and :765-776), which forms C as (sum of mi^2) - r2, one
+// rounding more than the fused path's chain from -r2; everything else is the same.
 template <int D>
 __device__ __forceinline__ void free_interval(const double* x, const double* a, const double* di,
                                               double A, double inv2A, double r2, double& lo,
-                                              double& hi) {
-  double B = 0.0, Cc = -r2;
+                                              double& hi, bool mat = false) {
+  double B = 0.0, Cc = mat ? 0.0 : -r2;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
     const double mi = __dsub_rn(a[k], x[k]);
     B = __fma_rn(mi, di[k], B);
     Cc = __fma_rn(mi, mi, Cc);
   }
+  if (mat) Cc = __dsub_rn(Cc, r2);
   B = __dmul_rn(B, 2.0);
   const double disc = __fma_rn(B, B, -__dmul_rn(__dmul_rn(4.0, A), Cc));
   lo = -1.0;
@@ -329,7 +333,7 @@ __device__ __forceinline__ void load_col(const PairDesc& pd, int j, ColRec<KIND,
 template <int KIND, int D>
 __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<KIND, D>& col, int i,
                                      int j, double left, double& bot, double& carry, double r2,
-                                     double& res, bool last, bool tr = false) {
+                                     double& res, bool last, bool tr = false, bool mat = false) {
   if (KIND == K_DFD) {
     const double dist = dist_sq<D>(row.a, col.qa);
     if (i == 0) {
@@ -362,8 +366,8 @@ __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<K
       if (last) res = fmin(top, right);
     } else {
       double rLB, rUB, tLB, tUB;
-      free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);  // right edge
-      free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB); // top edge
+      free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB, mat);  // right edge
+      free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB, mat); // top edge
       const double leftLB = left, botLB = bot;
       if (botLB < 0.0) {
         const bool invalid = (leftLB > rUB) || (leftLB < 0.0);
@@ -439,6 +443,7 @@ __device__ StripOut run_strip(const WaveArgs& wa, const PairDesc& pd, PairState*
   const unsigned E = st->epoch;
   const double U = st->U;
   const double r2 = st->r2;
+  const bool mat = st->formula == 1;
   const bool dense = KIND == K_DFD || st->dense != 0;  // DFD runs unpruned (U = +inf)
   const bool has_prod = s > 0;
   const bool has_cons = s + 1 < S;
@@ -629,7 +634,7 @@ __device__ StripOut run_strip(const WaveArgs& wa, const PairDesc& pd, PairState*
       if (__any_sync(kFull, need)) {
         if (act) {
           cell<KIND, D>(row, cur, i, j, left, bot, carry, r2, res, last_row && j == C - 1,
-                        pd.tr != 0);
+                        pd.tr != 0, mat);
           ++evaluated;
         }
       } else if (act) {

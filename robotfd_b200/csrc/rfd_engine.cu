@@ -909,6 +909,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     return fail(RFD_ERR_ARG, "coarse_ub must be 0 or in [2, 4096]");
   if (o.coarse_ub && o.reference_quirks)
     return fail(RFD_ERR_ARG, "coarse_ub needs reference_quirks = 0 (the quirk reads the DFD sizes)");
+  if (o.formula < RFD_FORMULA_FUSED || o.formula > RFD_FORMULA_REFERENCE)
+    return fail(RFD_ERR_ARG, "formula");
+  if (o.formula != RFD_FORMULA_FUSED && o.precision == RFD_PREC_FP32_FILTER)
+    return fail(RFD_ERR_ARG, "the FP32 filter certifies the fused formula's intervals only");
   for (int64_t p = 0; p < npairs; ++p) {
     int rc = check_pair(c1s[p], n1s[p], c2s[p], n2s[p], dims[p]);
     if (rc) return rc;
@@ -963,6 +967,27 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
     n1s = kept1.data();
     n2s = kept2.data();
+  }
+
+  // decision formula per pair: RFD_FORMULA_REFERENCE takes the materialised path where the
+  // reference would, i.e. where its interval arrays fit in this device's free memory
+  // (src/intersection_algorithm_in_parallel.cu:87-97: maxThreadsPerBlock x SMs bytes plus
+  // 4 arrays of (n1-1)(n2-2+n1-2)+n1 doubles)
+  std::vector<int> formula((size_t)npairs, o.formula == RFD_FORMULA_MATERIALISED ? 1 : 0);
+  if (o.formula == RFD_FORMULA_REFERENCE) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    int mtpb = 1024;
+    cudaDeviceGetAttribute(&mtpb, cudaDevAttrMaxThreadsPerBlock, ctx->device);
+    for (int64_t p = 0; p < npairs; ++p) {
+      const double a = (double)n1s[p];
+      const double need = (double)ctx->num_sms * (double)mtpb +
+                          ((a - 1.0) * ((double)n2s[p] - 2.0 + a - 2.0) + a) * 8.0 * 4.0;
+      formula[p] = (double)fr >= need ? 1 : 0;
+    }
   }
 
   // ---------------- layout
@@ -1178,6 +1203,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     s.filter = o.precision == RFD_PREC_FP32_FILTER ? 1 : 0;
     s.blo = s.bhi = NAN;
     s.coarse = (ck && n1 >= 2 && n2 >= 2) ? 1 : 0;
+    s.formula = formula[p];
     if (o.bracket && mode == MODE_DISTANCE) {
       s.blo = o.bracket[2 * p];
       s.bhi = o.bracket[2 * p + 1];
@@ -1494,6 +1520,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     mix(n1s, sizeof(int64_t) * npairs);
     mix(n2s, sizeof(int64_t) * npairs);
     mix(dims, sizeof(int32_t) * npairs);
+    mix(formula.data(), sizeof(int) * formula.size());
   }
   if (use_graph && ctx->gexec && ctx->gkey == key) {
     RFD_CUDA(cudaGraphLaunch(ctx->gexec, st));
@@ -1990,12 +2017,20 @@ int32_t rfd_bounds(rfd_context* ctx, const double* c1, int64_t n1, const double*
 
 int32_t rfd_decide(rfd_context* ctx, const double* c1, int64_t n1, const double* c2, int64_t n2,
                    int32_t dims, double radius, int32_t dense, int32_t* reachable, double* right_ub) {
+  return rfd_decide_formula(ctx, c1, n1, c2, n2, dims, radius, dense, RFD_FORMULA_FUSED, reachable,
+                            right_ub);
+}
+
+int32_t rfd_decide_formula(rfd_context* ctx, const double* c1, int64_t n1, const double* c2,
+                           int64_t n2, int32_t dims, double radius, int32_t dense, int32_t formula,
+                           int32_t* reachable, double* right_ub) {
   if (!ctx || !reachable) return fail(RFD_ERR_ARG, "null argument");
   if (!(radius >= 0.0)) return fail(RFD_ERR_ARG, "radius");
   RFD_CUDA(cudaSetDevice(ctx->device));
   rfd_options o;
   rfd_options_init(&o, 0);
   o.dense = dense;
+  o.formula = formula;
   rfd_result r;
   int rc = run_batch(ctx, 1, &c1, &n1, &c2, &n2, &dims, &o, &r, MODE_DECIDE, radius);
   if (rc) return rc;

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "frechet.hpp"
 #include "intersection_algorithm_in_parallel.hpp"
 #include "rfd.h"
@@ -62,7 +64,6 @@ namespace Frechet {
 namespace Continuous {
 
 double distance_cuda(const Curve& curve1, const Curve& curve2, const double eps, bool forceOversize) {
-  (void)forceOversize;
   std::printf("%ld, %ld\n", (long)curve1.size(), (long)curve2.size());
   const unsigned d = curve_dims(curve1);
   if (curve1.empty() || curve2.empty() || (d != 2 && d != 3) || curve_dims(curve2) != d) {
@@ -76,6 +77,8 @@ double distance_cuda(const Curve& curve1, const Curve& curve2, const double eps,
   rfd_options o;
   rfd_options_init(&o, 0);
   o.tol = eps;
+  // the reference's path choice: the fused kernel when forced, else by free device memory
+  o.formula = forceOversize ? RFD_FORMULA_FUSED : RFD_FORMULA_REFERENCE;
   rfd_result r;
   int rc = rfd_distance(ctx, a.data(), (int64_t)curve1.size(), b.data(), (int64_t)curve2.size(),
                         (int32_t)d, &o, &r);
@@ -141,7 +144,26 @@ Cuda_intersection::Cuda_intersection(const Curve& curve1, const Curve& curve2, b
     : intervalTime(0.0), reachTime(0.0), curve1_size((int)curve1.size()),
       curve2_size((int)curve2.size()), oversize(true), point_dimensions(curve_dims(curve1)),
       points_curve1_p(nullptr), points_curve2_p(nullptr), ctx(nullptr) {
-  if (forceOversize) *forceOversize = true;  // the fused O(n+m) decision is the only path
+  // The reference's choice of decision path (src/intersection_algorithm_in_parallel.cu:87-97):
+  // fused ("oversize") when forced or when its materialised interval arrays would not fit in
+  // free device memory, reported back through *forceOversize.  Here only the rounding of the
+  // free intervals follows the choice; the decision's memory is O(n+m) either way.
+  oversize = forceOversize ? *forceOversize : false;
+  if (!oversize) {
+    size_t fr = 0, tot = 0;
+    int dev = 0, sms = 0, mtpb = 1024;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaMemGetInfo(&fr, &tot) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&mtpb, cudaDevAttrMaxThreadsPerBlock, dev) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    const double a = (double)curve1_size;
+    const double need = (double)sms * (double)mtpb +
+                        ((a - 1.0) * ((double)curve2_size - 2.0 + a - 2.0) + a) * 8.0 * 4.0;
+    oversize = !((double)fr >= need);
+  }
+  if (forceOversize) *forceOversize = oversize;
   std::vector<double> a = flatten(curve1, point_dimensions), b = flatten(curve2, point_dimensions);
   points_curve1_p = (double*)std::malloc(sizeof(double) * (a.size() ? a.size() : 1));
   points_curve2_p = (double*)std::malloc(sizeof(double) * (b.size() ? b.size() : 1));
@@ -176,8 +198,10 @@ bool Cuda_intersection::intersection_interval_call_gpu(double radius) {
   if (!ctx || !points_curve1_p || !points_curve2_p) return false;
   auto t0 = std::chrono::high_resolution_clock::now();
   int32_t reach = 0;
-  int rc = rfd_decide(ctx, points_curve1_p, curve1_size, points_curve2_p, curve2_size,
-                      (int32_t)point_dimensions, radius, 0, &reach, nullptr);
+  int rc = rfd_decide_formula(ctx, points_curve1_p, curve1_size, points_curve2_p, curve2_size,
+                              (int32_t)point_dimensions, radius, 0,
+                              oversize ? RFD_FORMULA_FUSED : RFD_FORMULA_MATERIALISED, &reach,
+                              nullptr);
   auto t1 = std::chrono::high_resolution_clock::now();
   reachTime += std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count() / 1000.0;
   if (rc) {

@@ -132,6 +132,7 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
   const bool rowv = i < R;
   const double r2 = st->r2;
   const bool filt = KIND == K_DEC && st->filter;  // FP32 classification first (rfd_filter.h)
+  const bool mat = KIND == K_DEC && st->formula == 1;  // materialised path's intervals
   RowData<KIND, D> row;
   if (rowv) row.load(pd, i);
   const long long t0 = clock64();
@@ -207,13 +208,13 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
           ct = interval_class32<D>(col.qb, row.a, row.ab, row.A, r2);
         }
         if (cr == 0) {
-          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB);
+          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB, mat);
         } else {
           rLB = cr == 1 ? -1.0 : 0.0;
           rUB = cr == 1 ? -2.0 : 1.0;
         }
         if (ct == 0) {
-          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB);
+          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB, mat);
         } else {
           tLB = ct == 1 ? -1.0 : 0.0;
           tUB = ct == 1 ? -2.0 : 1.0;

@@ -132,9 +132,14 @@ def test_degenerate_single_point(ctx):
 
 
 def test_compute_distance_parallel_mirror(ctx, built):
+    """The reference's entry point: its stop rule and VE-FD rule, and its decision path - the
+    materialised intervals where they fit in device memory (always at this size), the fused
+    kernel's when forceOversize is set."""
     P, Q = walk_pair(5, 150, 120, 2)
-    want = oracle.distance(P, Q, stop_mode=0, quirks=True)
+    want = oracle.distance(P, Q, stop_mode=0, quirks=True, formula=1)
     assert built.compute_distance_parallel(P, Q) == want["distance"]
+    want = oracle.distance(P, Q, stop_mode=0, quirks=True, formula=0)
+    assert built.compute_distance_parallel(P, Q, force_oversize=True) == want["distance"]
 
 
 @pytest.mark.parametrize("style,d,n", [(1, 3, 20000), (0, 2, 12000), (1, 2, 30000)])

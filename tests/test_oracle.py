@@ -146,3 +146,33 @@ def test_reference_stop_rule_and_quirk():
     r2 = oracle.distance(P, Q, stop_mode=0, quirks=False)
     assert r2["vefd"] >= r["vefd"]
     assert abs(r2["distance"] - r["distance"]) <= oracle.FLT_EPSILON
+
+
+def test_materialised_formula_rounds_differently():
+    """The reference's two decision paths round C of the quadratic differently: the
+    materialised path forms (sum mi^2) - r^2 (src/intersection_algorithm_in_parallel.cu:742),
+    the fused one sums from -r^2 (.cu:1177-1186).  Their intervals differ in the last bits for
+    some partial edges, never by more than a few ulps of the edge parameter, and agree on
+    emptiness away from tangency."""
+    rng = np.random.default_rng(7)
+    n = 50000
+    X = rng.normal(size=(n, 3)) * 100.0
+    a = X + rng.normal(size=(n, 3))
+    b = a + rng.normal(size=(n, 3))
+    A = ((b - a) ** 2).sum(1)
+    r2 = float(np.median(((a - X) ** 2).sum(1)))
+    l0, h0 = oracle.free_intervals(X, a, b, A, r2)
+    l1, h1 = oracle.free_intervals(X, a, b, A, r2, formula=1)
+    part = (l0 >= 0) & (l1 >= 0)
+    assert (l0 != l1).sum() + (h0 != h1).sum() > 100
+    assert np.max(np.abs(l0[part] - l1[part])) < 1e-9
+    assert np.max(np.abs(h0[part] - h1[part])) < 1e-9
+    assert ((l0 < 0) != (l1 < 0)).sum() < 5
+
+
+def test_materialised_search_close_to_fused():
+    P, Q = oracle.gen_pair(1, 3, 400, 350, 100.0, 0.1, 8, 0)
+    a = oracle.distance(P, Q, stop_mode=1, quirks=False)
+    b = oracle.distance(P, Q, stop_mode=1, quirks=False, formula=1)
+    assert abs(a["distance"] - b["distance"]) <= 2.0 ** -32 * a["distance"]
+    assert a["vefd"] == b["vefd"] and a["dfd"] == b["dfd"]
