@@ -60,12 +60,13 @@ struct Prog {
 // stored are set back to "not yet written" first (kBndEmpty), because a reader takes a word
 // that is not kBndEmpty as final.  The slot word of each ring row says whose row it is now:
 //   team strips (VE-FD, decisions; rfd_team.cuh): (epoch << 32) | owner, the strip that
-//     claimed the row for its output (kSlotFresh: nobody since the phase began).  A strip
-//     claims its row at its start: it waits until the previous owner o and strip o + 1 have
-//     ended (Prog.done), clears the words and tags o and earlier owners wrote (the row's
-//     dirty chunk range, slot_dirty), and releases the slot word with its own index.  Its
-//     reader waits for that before reading the row.  A strip known dead at its start writes
-//     nothing and claims nothing.
+//     claimed the row for its output (kSlotFresh: nobody since the phase began).  A strip s
+//     claims its row at its start, in strip order: it waits until strip o = s - ring holds
+//     the row and until o and strip o + 1 have ended (Prog.done), clears the words and tags
+//     written since the row was last cleared (its dirty chunk range, slot_dirty), and
+//     releases the slot word with its own index.  Its reader waits for that before reading
+//     the row.  A strip known dead at its start writes nothing and claims nothing (every
+//     later strip is dead as well).
 //   DFD strips (rfd_dfd.cuh): (next writer << 32) | columns cleared for it.  The reader of a
 //     row clears each chunk right after reading it and releases the count every few chunks;
 //     the next writer of the row writes a column only once it is cleared, and that writer's

@@ -323,21 +323,23 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     out_prog->first_live = kNone;
     out_prog->last_live = 0;
   }
-  // Claim of the output row: wait until its previous owner o and o's reader (strip o + 1)
-  // have ended, set the words and tags stored since the row was last cleared back to "not
-  // yet written", then publish this strip as the owner.  Returns 0, 1 (strip known dead:
-  // it will write nothing) or 2 (error / timeout).
+  // Claim of the output row.  A row's owners claim it in strip order: strip s takes it from
+  // strip o = s - ring (s < ring: a fresh row).  Wait until o holds it (a dead o never claims,
+  // but then this strip is dead too), then until o and o's reader (strip o + 1) have ended,
+  // set the words and tags stored since the row was last cleared back to "not yet written",
+  // and publish this strip as the owner.  Returns 0, 1 (strip known dead: it will write
+  // nothing) or 2 (error / timeout).
   bool claimed = false;
   auto claim = [&]() -> int {
     unsigned long long* sw = pd.slots + slot_out;
-    const unsigned long long w = bcast(lane == 0 ? ld_acquire(sw) : 0ull);
-    const unsigned owner = (unsigned)(w & 0xffffffffu);
-    if ((unsigned)(w >> 32) != E) {  // every phase sets its slot words before its strips run
-      if (lane == 0) atomicExch(wa.error, 1);
-      return 2;
+    const int o = s - pd.ring;
+    const unsigned long long held = ((unsigned long long)E << 32) | (o >= 0 ? (unsigned)o : kSlotFresh);
+    for (int it = 0;; ++it) {
+      if (bcast(lane == 0 ? ld_acquire(sw) : 0ull) == held) break;
+      const int r = wt.check(it);
+      if (r) return r;
     }
-    if (owner != kSlotFresh) {
-      const int o = (int)owner;
+    if (o >= 0) {
       const unsigned long long fin = ((unsigned long long)E << 32) | 1ull;
       for (int it = 0;; ++it) {
         int ok = 0;
