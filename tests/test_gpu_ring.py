@@ -65,7 +65,7 @@ def test_small_dfd_ring_every_tile_shape(built, rows, skew):
         for n1, n2, d in ((32 * 8 * int(rows) * 3 + 5, 900, 2), (1500, 2100, 3)):
             P, Q = built.gen_pair(1, d, n1, n2, 100.0, 0.1, 32, n1)
             dfd, _ = c.bounds(P, Q, quirks=False)
-            assert dfd * dfd == oracle.dfd_sq(P, Q, oracle.max_threads()), (n1, n2, d)
+            assert dfd == np.sqrt(oracle.dfd_sq(P, Q, oracle.max_threads())), (n1, n2, d)
     finally:
         c.close()
 

@@ -79,6 +79,6 @@ def test_environment_sets_the_budget_of_new_contexts(built, monkeypatch):
     c = built.Context(0)
     try:
         dfd, vefd = c.bounds(P, Q, quirks=False)
-        assert dfd * dfd == oracle.dfd_sq(P, Q)
+        assert dfd == oracle.dfd_sq(P, Q) ** 0.5
     finally:
         c.close()
