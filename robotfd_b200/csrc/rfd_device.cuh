@@ -391,6 +391,15 @@ __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<K
 
 // ------------------------------------------------------------------ waits
 
+// Self-checks of the boundary ring's indices: a failed check records its code in the error
+// word (codes from kCheckBase; the call then fails with RFD_ERR_INTERNAL) and the access is
+// skipped.
+constexpr int kCheckBase = 16;
+__device__ __forceinline__ bool ring_check(const WaveArgs& wa, bool ok, int code) {
+  if (!ok) atomicCAS(wa.error, 0, kCheckBase + code);
+  return ok;
+}
+
 // Broadcast lane 0's value: every value that steers control flow is read by lane 0 only
 // and shared, so all 32 lanes always take the same branch around full-mask shuffles.
 __device__ __forceinline__ int bcast(int v) { return __shfl_sync(kFull, v, 0); }

@@ -85,6 +85,8 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   const int slot_out = has_cons ? s % nring : 0;
   double* in_bnd = has_prod ? pd.bnd + (size_t)slot_in * pd.cstride : nullptr;
   double* out_bnd = has_cons ? pd.bnd + (size_t)slot_out * pd.cstride : nullptr;
+  if (!ring_check(wa, slot_in >= 0 && slot_in < nring && slot_out >= 0 && slot_out < nring, 8))
+    return 1;
   unsigned long long* in_slot = pd.slots + slot_in;
   unsigned long long* out_slot = pd.slots + slot_out;
   unsigned in_ok = 0, out_ok = 0;  // leading columns cleared for the input's / this strip's writer

@@ -581,7 +581,9 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
       const unsigned E2 = *(volatile unsigned*)&st->epoch;
       const int nrows = S > 1 ? min(pd.ring, S - 1) : 0;
       for (int r = warp; r < nrows; r += kTeamThreads / 32) {
-        const int2 d = ld_volatile(pd.slot_dirty + r);
+        int2 d = ld_volatile(pd.slot_dirty + r);
+        if (!ring_check(wa, d.x > d.y || (d.x >= 0 && ((long long)d.y << 5) < C + 32), 7))
+          d = make_int2(INT_MAX, -1);
         double* row = pd.bnd + (size_t)r * pd.cstride;
         const long long end = min((long long)(d.y + 1) << 5, C);
         for (long long w = ((long long)d.x << 5) + lane; d.x <= d.y && w < end; w += 32)
@@ -1555,6 +1557,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   RFD_CUDA(cudaStreamSynchronize(st));
+  if (hmisc[1] >= kCheckBase)
+    return fail(RFD_ERR_INTERNAL, "device self-check " + std::to_string(hmisc[1] - kCheckBase) +
+                                      " failed (boundary ring index out of range)");
   if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
   if (ctx->prof) {
     std::vector<unsigned long long> pc(kTraceBase + 3 * kTrace);

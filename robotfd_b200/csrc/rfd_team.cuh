@@ -331,8 +331,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // nothing) or 2 (error / timeout).
   bool claimed = false;
   auto claim = [&]() -> int {
+    if (!ring_check(wa, slot_out >= 0 && slot_out < pd.ring, 1)) return 2;
     unsigned long long* sw = pd.slots + slot_out;
     const int o = s - pd.ring;
+    if (!ring_check(wa, o < S, 2)) return 2;
     const unsigned long long held = ((unsigned long long)E << 32) | (o >= 0 ? (unsigned)o : kSlotFresh);
     for (int it = 0;; ++it) {
       if (bcast(lane == 0 ? ld_acquire(sw) : 0ull) == held) break;
@@ -355,6 +357,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       if (lane == 0) dr = ld_volatile(pd.slot_dirty + slot_out);
       dr.x = bcast(dr.x);
       dr.y = bcast(dr.y);
+      if (!ring_check(wa, dr.x > dr.y || (dr.x >= 0 && dr.y < nout), 3)) return 2;
       for (int k = dr.x; k <= dr.y; ++k) {
         const int col = (k << 5) + lane;
         if (col < C) st_relaxed_u64(reinterpret_cast<unsigned long long*>(out_bnd) + col, kBndEmpty);
@@ -382,6 +385,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // The reader's side: the input row is read only once its producer owns it (before that it
   // may hold an earlier owner's words).
   bool in_ok = !has_prod;
+  if (has_prod && !ring_check(wa, slot_in >= 0 && slot_in < pd.ring, 6)) status = 1;
   auto wait_in = [&]() -> int {
     const unsigned long long want = ((unsigned long long)E << 32) | (unsigned)(s - 1);
     for (int it = 0;; ++it) {
@@ -440,6 +444,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // in-band flushes publish every 8th chunk and skip the fence's round trip otherwise.
   auto flush = [&](int k, bool publish) {
     const long long tf0 = wa.prof ? clock64() : 0;
+    if (!ring_check(wa, k >= 0 && k < nout && claimed, 4)) return;  // (k, claimed: warp-uniform)
     const int col = (k << 5) + lane;
     __syncwarp();
     const double v = out_row[((k & 1) << 5) + lane];
@@ -779,7 +784,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     out_prog->wlo = wlo;
     out_prog->whi = whi;
     // what this strip stored stays recorded against the row until the next owner clears it
-    if (claimed && wlo <= whi) {
+    if (claimed && wlo <= whi && ring_check(wa, wlo >= 0 && whi < nout, 5)) {
       int2* dp = pd.slot_dirty + slot_out;
       const int2 d = ld_volatile(dp);
       st_volatile(dp, make_int2(min(d.x, wlo), max(d.y, whi)));
