@@ -50,29 +50,17 @@ struct Prog {
   unsigned int first_live;  // first chunk holding a live value (kNone while none)
   unsigned int last_live;   // last such chunk
   int wlo, whi;             // chunks of the strip's output row it wrote (wlo > whi: none)
-  unsigned long long done;  // (epoch << 32) | 1 once the strip has ended (team strips)
 };
 
-// Boundary ring.  The rows strips hand to each other live in a ring of `ring` rows per pair,
-// not one row per strip: strip s writes row s % ring, so the boundary memory is O(ring *
-// columns), independent of the number of rows.  A row is reused only when its previous
-// writer and that writer's reader are finished with it, and the words its previous writer
-// stored are set back to "not yet written" first (kBndEmpty), because a reader takes a word
-// that is not kBndEmpty as final.  The slot word of each ring row says whose row it is now:
-//   team strips (VE-FD, decisions; rfd_team.cuh): (epoch << 32) | owner, the strip that
-//     claimed the row for its output (kSlotFresh: nobody since the phase began).  A strip s
-//     claims its row at its start, in strip order: it waits until strip o = s - ring holds
-//     the row and until o and strip o + 1 have ended (Prog.done), clears the words and tags
-//     written since the row was last cleared (its dirty chunk range, slot_dirty), and
-//     releases the slot word with its own index.  Its reader waits for that before reading
-//     the row.  A strip known dead at its start writes nothing and claims nothing (every
-//     later strip is dead as well).
-//   DFD strips (rfd_dfd.cuh): (next writer << 32) | columns cleared for it.  The reader of a
-//     row clears each chunk right after reading it and releases the count every few chunks;
-//     the next writer of the row writes a column only once it is cleared, and that writer's
-//     reader trusts a word only where the count covers it.  The DFD's strips all run the
-//     full width at once, so the row is handed on column by column, not as a whole.
-constexpr unsigned kSlotFresh = 0xffffffffu;
+// Boundary ring of the DFD strips.  The rows DFD strips hand to each other live in a ring of
+// `ring` rows per pair, not one row per strip: strip s writes row s % ring, so their boundary
+// memory is O(ring * columns), independent of the number of rows.  Each ring row has a slot
+// word, (next writer << 32) | columns cleared for it.  The reader of a row sets each chunk
+// back to "not yet written" (kBndEmpty: a reader takes any other word as final) right after
+// reading it and releases the cleared count every few chunks; the row's next writer writes a
+// column only once it is cleared, and that writer's reader trusts a word only where the count
+// covers it.  The DFD's strips all run the full width at once, so the row is handed on column
+// by column, not as a whole.  (VE-FD and decision strips keep one row per strip.)
 constexpr unsigned kSlotAll = 0xffffffffu;  // DFD slot word: every column cleared
 
 struct PairDesc {
@@ -80,12 +68,11 @@ struct PairDesc {
   const double* Q;        // curve 2, [n2][d]
   const double2* rowc;    // [n1-1]: (|p_{i+1}-p_i|^2, 0.5 / that)
   const double2* colrec;  // [n2-1][RECW(d)]: q_j, q_{j+1}, (|q_{j+1}-q_j|^2, 0.5 / that)
-  double* bnd;            // [ring][cstride] boundary rows (strip s writes row s % ring)
-  unsigned int* tags;     // [ring][tstride] epoch tag of every live chunk (team strips)
+  double* bnd;            // boundary rows: [S-1][cstride] (team strips), [ring][cstride] (DFD)
+  unsigned int* tags;     // [S-1][tstride] epoch tag of every live chunk (team strips)
   Prog* prog;             // [S]
-  unsigned long long* slots;  // [ring] slot word of every ring row (see Boundary ring)
-  int2* slot_dirty;           // [ring] chunks written since the row was last cleared (team)
-  int ring;                   // rows of the ring (>= 1; strips' rows never wrap when >= S-1)
+  unsigned long long* slots;  // [ring] slot word of every DFD ring row (see Boundary ring)
+  int ring;                   // rows of the DFD ring (>= 1; rows never wrap when >= S-1)
   // tr: the team strips of a pair whose first curve is the longer run on the transposed
   // grid (rows = curve 2), whose free intervals are the same values (the interval of an edge
   // is the same function of its point and segment in either orientation) with the roles of
@@ -155,15 +142,6 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
-__device__ __forceinline__ int2 ld_volatile(const int2* p) {
-  const volatile int* q = reinterpret_cast<const volatile int*>(p);
-  return make_int2(q[0], q[1]);
-}
-__device__ __forceinline__ void st_volatile(int2* p, int2 v) {
-  volatile int* q = reinterpret_cast<volatile int*>(p);
-  q[0] = v.x;
-  q[1] = v.y;
-}
 
 // Boundary rows are filled with this pattern before every launch that hands rows between
 // strips (a NaN that no DP value takes: arithmetic makes canonical NaNs), so a consumer can
@@ -391,9 +369,9 @@ __device__ __forceinline__ void cell(const RowData<KIND, D>& row, const ColRec<K
 
 // ------------------------------------------------------------------ waits
 
-// Self-checks of the boundary ring's indices: a failed check records its code in the error
-// word (codes from kCheckBase; the call then fails with RFD_ERR_INTERNAL) and the access is
-// skipped.
+// Self-check of the DFD boundary ring's indices: a failed check records its code in the error
+// word (codes from kCheckBase; the call then fails with RFD_ERR_INTERNAL) and the strip does
+// not touch the ring.
 constexpr int kCheckBase = 16;
 __device__ __forceinline__ bool ring_check(const WaveArgs& wa, bool ok, int code) {
   if (!ok) atomicCAS(wa.error, 0, kCheckBase + code);

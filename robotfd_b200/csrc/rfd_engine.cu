@@ -38,12 +38,8 @@ namespace {
 
 constexpr int kBlock = 128;
 
-// Boundary ring rows per pair.  Team strips: a decision's or VE-FD's band keeps only the
-// strips it passes through busy, and a strip claims a row only from a strip that ended, so
-// the ring holds the strips in flight with a wide margin (a band of w columns keeps about
-// w / 190 strips busy at once).  DFD strips hand rows on column by column and need only a few
-// strips' lag: kPublish chunks plus the publication's latency.
-constexpr int kTeamRingRows = 128;
+// Boundary ring rows per pair of the DFD strips, which hand rows on column by column and
+// need only a few strips' lag: kPublish chunks plus the publication's latency.
 constexpr int kDfdRingRows = 32;
 thread_local std::string g_last_error;
 
@@ -379,19 +375,10 @@ __global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int 
     const PairDesc pd = pairs[p];
     const long long S = (pd.n1 - 1 + 31) / 32;
     if (S < 2) continue;
-    const long long rows = min(S - 1, (long long)pd.ring);
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
-    const long long n = rows * pd.cstride / 2;
+    const long long n = (S - 1) * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
       b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
-    // every ring row fresh for this phase's epoch, nothing written to it yet
-    if (blockIdx.x == 0) {
-      const unsigned E = st[p].epoch;
-      for (int k = threadIdx.x; k < rows; k += blockDim.x) {
-        pd.slots[k] = ((unsigned long long)E << 32) | kSlotFresh;
-        pd.slot_dirty[k] = make_int2(INT_MAX, -1);
-      }
-    }
   }
 }
 
@@ -575,24 +562,14 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
     }
     __syncthreads();
     if (KIND == K_DEC && sh->push) {
-      // the ring rows' written words back to "not yet written" and every row fresh for the
-      // next probe's epoch (its tags are told apart by the epoch), one row per warp
+      // the probe's written boundary words back to "not yet written", one strip per warp
       const long long C = pd.n2 - 1;
-      const unsigned E2 = *(volatile unsigned*)&st->epoch;
-      const int nrows = S > 1 ? min(pd.ring, S - 1) : 0;
-      for (int r = warp; r < nrows; r += kTeamThreads / 32) {
-        int2 d = ld_volatile(pd.slot_dirty + r);
-        if (!ring_check(wa, d.x > d.y || (d.x >= 0 && ((long long)d.y << 5) < C + 32), 7))
-          d = make_int2(INT_MAX, -1);
+      for (int r = warp; r < S - 1; r += kTeamThreads / 32) {
+        const int lo = pd.prog[r].wlo, hi = pd.prog[r].whi;
         double* row = pd.bnd + (size_t)r * pd.cstride;
-        const long long end = min((long long)(d.y + 1) << 5, C);
-        for (long long w = ((long long)d.x << 5) + lane; d.x <= d.y && w < end; w += 32)
+        const long long end = min((long long)(hi + 1) << 5, C);
+        for (long long w = ((long long)lo << 5) + lane; lo <= hi && w < end; w += 32)
           reinterpret_cast<unsigned long long*>(row)[w] = kBndEmpty;
-        __syncwarp();
-        if (lane == 0) {
-          st_volatile(pd.slot_dirty + r, make_int2(INT_MAX, -1));
-          pd.slots[r] = ((unsigned long long)E2 << 32) | kSlotFresh;
-        }
       }
       __threadfence();
       __syncthreads();
@@ -743,9 +720,8 @@ struct rfd_context {
   int dfd_grid_all[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // for rows 1, 2, 4, 8
   int dfd_grid_infl[2] = {0, 0};  // inflated coarse sweep, 1 row per lane
   int prof = 0;  // RFD_PROF=1: team-strip cycle counters printed to stderr after each call
-  // rows of the boundary ring per pair (see "Boundary ring" in rfd_device.cuh): team strips
-  // (RFD_RING_ROWS) and DFD strips (RFD_DFD_RING_ROWS); at least 2
-  int ring_rows = kTeamRingRows;
+  // rows of the DFD strips' boundary ring per pair (RFD_DFD_RING_ROWS, at least 2; see
+  // "Boundary ring" in rfd_device.cuh)
   int dfd_ring_rows = kDfdRingRows;
   void* dws = nullptr;
   size_t dws_size = 0;
@@ -831,7 +807,7 @@ struct Layout {
   // device offsets
   size_t descs, tdescs, states, items, titems, counters, error, active, zero_begin, zero_end,
       total;
-  std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog, slots, dirty;
+  std::vector<size_t> P, Q, rowc, colrec, bnd, tags, prog, slots;
   std::vector<int> ring_d, ring_t, ring_c;  // ring rows: DFD, team strips, coarse DFD
   // host staging offsets
   size_t h_descs, h_tdescs, h_states, h_items, h_titems, h_misc, h_curves, h_total;
@@ -840,12 +816,12 @@ struct Layout {
 };
 
 // Device workspace of one pair in a batch (an upper bound of what run_batch lays out for
-// it): curves, segment records, the boundary ring, tags, progress and slot words, items.
+// it): curves, segment records, boundary rows (the team strips' n1 n2 / 4 bytes dominate),
+// tags, progress and slot words, items.
 double pair_workspace_bytes(const rfd_context* ctx, int64_t n1, int64_t n2, int d, int ck) {
   const int64_t rows = std::min(n1, n2), cols = std::max(n1, n2);
   const int64_t St = (std::max<int64_t>(rows - 1, 0) + 31) / 32;
-  const double rt = ctx->solo ? (double)std::max<int64_t>(St - 1, 1)
-                              : (double)ring_of(St, ctx->ring_rows);
+  const double rt = (double)std::max<int64_t>(St - 1, 1);  // team strips: a row per strip
   const double rd = (double)ring_of((n1 + 31) / 32, ctx->dfd_ring_rows);
   const double ring_words = std::max(rt * (double)(cols + 32), rd * (double)(n2 + 32));
   double b = 8.0 * (double)d * (double)(n1 + n2)         // curves
@@ -996,7 +972,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   Layout L;
   L.P.resize(npairs); L.Q.resize(npairs); L.rowc.resize(npairs); L.colrec.resize(npairs);
   L.bnd.resize(npairs); L.tags.resize(npairs); L.prog.resize(npairs);
-  L.slots.resize(npairs); L.dirty.resize(npairs);
+  L.slots.resize(npairs);
   L.ring_d.resize(npairs); L.ring_t.resize(npairs); L.ring_c.resize(npairs);
   L.hP.resize(npairs); L.hQ.resize(npairs);
   const int ck = mode == MODE_DISTANCE ? o.coarse_ub : 0;  // coarse upper bound, every ck-th point
@@ -1054,20 +1030,19 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {
-    // ring rows: team strips of 32 segment rows; DFD strips of at least 32 point rows (the
-    // strip height the autotuner may pick); the coarse pair's DFD
+    // boundary rows: team strips of 32 segment rows, one row each; the DFD ring for strips of
+    // at least 32 point rows (the strip height the autotuner may pick); the coarse pair's DFD
     const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
-    L.ring_t[p] = ctx->solo ? ring_of(St, INT32_MAX) : ring_of(St, ctx->ring_rows);
+    // team strips hand rows over through one row per strip (S - 1 rows)
+    L.ring_t[p] = ring_of(St, INT32_MAX);
     L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
     L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
                       ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
-    // progress words, tags (team strips) and slot words: cleared every call
+    // progress words, tags (team strips) and the DFD ring's slot words: cleared every call
     const int64_t tstride = align_up((size_t)((tcols(p) + 31) / 32), 32);
     L.tags[p] = take(sizeof(unsigned) * L.ring_t[p] * tstride);
     L.prog[p] = take(sizeof(Prog) * std::max<int64_t>(St, (trows(p) + 31) / 32));
-    L.slots[p] = take(sizeof(unsigned long long) *
-                      std::max(L.ring_t[p], std::max(L.ring_d[p], L.ring_c[p])));
-    L.dirty[p] = take(sizeof(int2) * L.ring_t[p]);
+    L.slots[p] = take(sizeof(unsigned long long) * std::max(L.ring_d[p], L.ring_c[p]));
   }
   L.zero_end = off;
   L.active = take(sizeof(int));
@@ -1160,7 +1135,6 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     D.tags = (unsigned*)(dbase + L.tags[p]);
     D.prog = (Prog*)(dbase + L.prog[p]);
     D.slots = (unsigned long long*)(dbase + L.slots[p]);
-    D.slot_dirty = (int2*)(dbase + L.dirty[p]);
     D.ring = L.ring_d[p];
     D.n1 = (int)n1;
     D.n2 = (int)n2;
@@ -1747,7 +1721,6 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     }
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
-    c->ring_rows = env_rows("RFD_RING_ROWS", kTeamRingRows);
     c->dfd_ring_rows = env_rows("RFD_DFD_RING_ROWS", kDfdRingRows);
   }
   // wait budget: about 20 s at the maximum SM clock, or RFD_SPIN_CYCLES
@@ -2161,7 +2134,6 @@ int32_t rfd_search_step(double* state, int32_t* istate, int32_t stop_mode, int32
 namespace {
 
 constexpr size_t kNoAllocBytes = (size_t)64 << 20;  // 64 MiB
-constexpr int kNoAllocRing = 32;  // boundary ring rows
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 struct NoAllocDevice {
@@ -2235,10 +2207,9 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
     }
   }
   const NoAllocDevice nd = g_noalloc[dev];
-  // layout inside the array (same records as the allocating path; the strips hand rows
-  // over through a ring of kNoAllocRing rows, so the array holds pairs of any row count)
+  // layout inside the array (same records as the allocating path: one boundary row per strip)
   const int64_t S = (n1 - 1 + 31) / 32;  // 32-row strips over the n1 - 1 segment rows
-  const int ring = ring_of(S, kNoAllocRing);
+  const int ring = ring_of(S, INT32_MAX);
   const int64_t cstride = (int64_t)align_up((size_t)n2, 32);
   const int64_t tstride = (int64_t)align_up((size_t)((n2 + 31) / 32), 32);
   size_t off = 0;
@@ -2251,8 +2222,6 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   const size_t o_error = take(sizeof(int));
   const size_t o_tags = take(sizeof(unsigned) * (size_t)ring * tstride);
   const size_t o_prog = take(sizeof(Prog) * S);
-  const size_t o_slots = take(sizeof(unsigned long long) * ring);
-  const size_t o_dirty = take(sizeof(int2) * ring);
   const size_t zero_end = off;
   const size_t o_active = take(sizeof(int));
   const size_t o_rowc = take(sizeof(double2) * (size_t)(n1 - 1));
@@ -2272,8 +2241,6 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   d.bnd = (double*)(base + o_bnd);
   d.tags = (unsigned*)(base + o_tags);
   d.prog = (Prog*)(base + o_prog);
-  d.slots = (unsigned long long*)(base + o_slots);
-  d.slot_dirty = (int2*)(base + o_dirty);
   d.ring = ring;
   d.n1 = (int)n1;
   d.n2 = (int)n2;

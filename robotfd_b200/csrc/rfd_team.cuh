@@ -293,13 +293,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
 
   Prog* in_prog = has_prod ? pd.prog + (s - 1) : nullptr;
   Prog* out_prog = has_cons ? pd.prog + s : nullptr;
-  // rows of the boundary ring (see "Boundary ring" in rfd_device.cuh)
-  const int slot_in = has_prod ? (s - 1) % pd.ring : 0;
-  const int slot_out = has_cons ? s % pd.ring : 0;
-  const double* in_bnd = has_prod ? pd.bnd + (size_t)slot_in * pd.cstride : nullptr;
-  double* out_bnd = has_cons ? pd.bnd + (size_t)slot_out * pd.cstride : nullptr;
-  const unsigned* in_tags = has_prod ? pd.tags + (size_t)slot_in * pd.tstride : nullptr;
-  unsigned* out_tags = has_cons ? pd.tags + (size_t)slot_out * pd.tstride : nullptr;
+  const double* in_bnd = has_prod ? pd.bnd + (size_t)(s - 1) * pd.cstride : nullptr;
+  double* out_bnd = has_cons ? pd.bnd + (size_t)s * pd.cstride : nullptr;
+  const unsigned* in_tags = has_prod ? pd.tags + (size_t)(s - 1) * pd.tstride : nullptr;
+  unsigned* out_tags = has_cons ? pd.tags + (size_t)s * pd.tstride : nullptr;
 
   int status = 0;
   Waiter wt;
@@ -323,81 +320,6 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     out_prog->first_live = kNone;
     out_prog->last_live = 0;
   }
-  // Claim of the output row.  A row's owners claim it in strip order: strip s takes it from
-  // strip o = s - ring (s < ring: a fresh row).  Wait until o holds it (a dead o never claims,
-  // but then this strip is dead too), then until o and o's reader (strip o + 1) have ended,
-  // set the words and tags stored since the row was last cleared back to "not yet written",
-  // and publish this strip as the owner.  Returns 0, 1 (strip known dead: it will write
-  // nothing) or 2 (error / timeout).
-  bool claimed = false;
-  auto claim = [&]() -> int {
-    if (!ring_check(wa, slot_out >= 0 && slot_out < pd.ring, 1)) return 2;
-    unsigned long long* sw = pd.slots + slot_out;
-    const int o = s - pd.ring;
-    if (!ring_check(wa, o < S, 2)) return 2;
-    const unsigned long long held = ((unsigned long long)E << 32) | (o >= 0 ? (unsigned)o : kSlotFresh);
-    for (int it = 0;; ++it) {
-      if (bcast(lane == 0 ? ld_acquire(sw) : 0ull) == held) break;
-      const int r = wt.check(it);
-      if (r) return r;
-    }
-    if (o >= 0) {
-      const unsigned long long fin = ((unsigned long long)E << 32) | 1ull;
-      for (int it = 0;; ++it) {
-        int ok = 0;
-        if (lane == 0)
-          ok = ld_acquire(&pd.prog[o].done) == fin &&
-               (o + 1 >= S || ld_acquire(&pd.prog[o + 1].done) == fin);
-        if (bcast(ok)) break;
-        const int r = wt.check(it);
-        if (r) return r;
-      }
-      __syncwarp();
-      int2 dr = make_int2(0, -1);
-      if (lane == 0) dr = ld_volatile(pd.slot_dirty + slot_out);
-      dr.x = bcast(dr.x);
-      dr.y = bcast(dr.y);
-      if (!ring_check(wa, dr.x > dr.y || (dr.x >= 0 && dr.y < nout), 3)) return 2;
-      for (int k = dr.x; k <= dr.y; ++k) {
-        const int col = (k << 5) + lane;
-        if (col < C) st_relaxed_u64(reinterpret_cast<unsigned long long*>(out_bnd) + col, kBndEmpty);
-      }
-      for (int k = dr.x + lane; k <= dr.y; k += 32) __stcg(out_tags + k, 0u);
-      __syncwarp();
-      if (lane == 0) {
-        st_volatile(pd.slot_dirty + slot_out, make_int2(INT_MAX, -1));
-        __threadfence();
-        st_release(sw, ((unsigned long long)E << 32) | (unsigned)s);
-      }
-    } else if (lane == 0) {
-      // a fresh row was cleared before the phase began: nothing to order
-      st_relaxed_u64(sw, ((unsigned long long)E << 32) | (unsigned)s);
-    }
-    __syncwarp();
-    claimed = true;
-    return 0;
-  };
-  if (has_cons && !dead_tail) {
-    const int r = claim();
-    if (r == 2) status = 1;
-    else if (r == 1) dead_tail = true;
-  }
-  // The reader's side: the input row is read only once its producer owns it (before that it
-  // may hold an earlier owner's words).
-  bool in_ok = !has_prod;
-  if (has_prod && !ring_check(wa, slot_in >= 0 && slot_in < pd.ring, 6)) status = 1;
-  auto wait_in = [&]() -> int {
-    const unsigned long long want = ((unsigned long long)E << 32) | (unsigned)(s - 1);
-    for (int it = 0;; ++it) {
-      if (bcast(lane == 0 ? ld_acquire(pd.slots + slot_in) : 0ull) == want) {
-        __syncwarp();  // every lane's reads of the row are ordered after the acquire
-        in_ok = true;
-        return 0;
-      }
-      const int r = wt.check(it);
-      if (r) return r;
-    }
-  };
   double bot;
   if (KIND == K_DEC) bot = i == 0 ? 0.0 : -1.0;
   else bot = i == 0 ? st->seed : kFltMax;
@@ -444,7 +366,6 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   // in-band flushes publish every 8th chunk and skip the fence's round trip otherwise.
   auto flush = [&](int k, bool publish) {
     const long long tf0 = wa.prof ? clock64() : 0;
-    if (!ring_check(wa, k >= 0 && k < nout && claimed, 4)) return;  // (k, claimed: warp-uniform)
     const int col = (k << 5) + lane;
     __syncwarp();
     const double v = out_row[((k & 1) << 5) + lane];
@@ -507,14 +428,14 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   bool seen_live = false;  // has a live input chunk reached this strip yet
   auto prefetch = [&](int k) {
     pre_c = -1;
-    if (!has_prod || !in_ok || (k << 5) >= C) return;
+    if (!has_prod || (k << 5) >= C) return;
     const int col = (k << 5) + lane;
     pre = col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dead_value<KIND>());
     pre_c = k;
   };
 
   int c = 0;
-  while (status == 0 && !dead_tail && (c << 5) < nsteps) {
+  while (!dead_tail && (c << 5) < nsteps) {
     if (has_cons)
       while (next_flush <= c - 2) {
         flush(next_flush, (next_flush & 7) == 7);
@@ -523,11 +444,6 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     double inreg = dead_value<KIND>();
     bool in_live = false;
     bool fast = false;
-    if (has_prod && (c << 5) < C && !in_ok) {
-      const int r = wait_in();
-      if (r == 2) { status = 1; break; }
-      if (r == 1) { dead_tail = true; break; }
-    }
     if (has_prod && (c << 5) < C) {
       // Poll the chunk's words themselves (and, alongside, the progress word): a complete
       // chunk is used as soon as it lands.  A chunk the progress word calls final while
@@ -783,20 +699,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   if (has_cons && lane == 0) {
     out_prog->wlo = wlo;
     out_prog->whi = whi;
-    // what this strip stored stays recorded against the row until the next owner clears it
-    if (claimed && wlo <= whi && ring_check(wa, wlo >= 0 && whi < nout, 5)) {
-      int2* dp = pd.slot_dirty + slot_out;
-      const int2 d = ld_volatile(dp);
-      st_volatile(dp, make_int2(min(d.x, wlo), max(d.y, whi)));
-    }
   }
   if (s == S - 1 && last_row) st->result = res;
-  // the strip has ended (reads of its input row included): its rows may be claimed again
-  __syncwarp();
-  if (lane == 0 && status == 0) {
-    __threadfence();
-    st_release(&pd.prog[s].done, ((unsigned long long)E << 32) | 1ull);
-  }
   if (wa.prof && lane == 0) atomicAdd(&wa.prof[4], (unsigned long long)(clock64() - t0));
   return status;
 }
