@@ -54,14 +54,15 @@ struct Prog {
 
 // Boundary ring of the DFD strips.  The rows DFD strips hand to each other live in a ring of
 // `ring` rows per pair, not one row per strip: strip s writes row s % ring, so their boundary
-// memory is O(ring * columns), independent of the number of rows.  Each ring row has a slot
-// word, (next writer << 32) | columns cleared for it.  The reader of a row sets each chunk
-// back to "not yet written" (kBndEmpty: a reader takes any other word as final) right after
-// reading it and releases the cleared count every few chunks; the row's next writer writes a
-// column only once it is cleared, and that writer's reader trusts a word only where the count
-// covers it.  The DFD's strips all run the full width at once, so the row is handed on column
-// by column, not as a whole.  (VE-FD and decision strips keep one row per strip.)
-constexpr unsigned kSlotAll = 0xffffffffu;  // DFD slot word: every column cleared
+// memory is O(ring * columns), independent of the number of rows.  A count per strip,
+// slots[s], says how many leading columns of its row have been cleared for it.  The reader of
+// a row sets each chunk back to "not yet written" (kBndEmpty: a reader takes any other word as
+// final) right after reading it and releases the count of the row's next writer every few
+// chunks; a writer writes a column only once it is cleared, and its reader trusts a word only
+// where its writer's count covers it.  The DFD's strips all run the full width at once, so a
+// row is handed on column by column, not as a whole.  (VE-FD and decision strips keep one row
+// per strip.)
+constexpr unsigned kSlotAll = 0xffffffffu;  // cleared count: every column
 
 struct PairDesc {
   const double* P;        // curve 1, [n1][d]
@@ -71,7 +72,7 @@ struct PairDesc {
   double* bnd;            // boundary rows: [S-1][cstride] (team strips), [ring][cstride] (DFD)
   unsigned int* tags;     // [S-1][tstride] epoch tag of every live chunk (team strips)
   Prog* prog;             // [S]
-  unsigned long long* slots;  // [ring] slot word of every DFD ring row (see Boundary ring)
+  unsigned long long* slots;  // [S] cleared count of every DFD strip (see Boundary ring)
   int ring;                   // rows of the DFD ring (>= 1; rows never wrap when >= S-1)
   // tr: the team strips of a pair whose first curve is the longer run on the transposed
   // grid (rows = curve 2), whose free intervals are the same values (the interval of an edge

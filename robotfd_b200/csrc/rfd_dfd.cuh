@@ -79,16 +79,19 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
   const bool has_cons = s + 1 < S;
   // rows of the boundary ring, handed on column by column (see "Boundary ring" in
   // rfd_device.cuh): this strip clears each input chunk once read, and writes an output column
-  // only where the row's previous reader has cleared it
+  // only where the row's previous reader has cleared it.  clr[w] counts the columns cleared
+  // for writer w; its one publisher is the reader of the row's previous writer.
   const int nring = pd.ring;
   const int slot_in = has_prod ? (s - 1) % nring : 0;
   const int slot_out = has_cons ? s % nring : 0;
-  double* in_bnd = has_prod ? pd.bnd + (size_t)slot_in * pd.cstride : nullptr;
-  double* out_bnd = has_cons ? pd.bnd + (size_t)slot_out * pd.cstride : nullptr;
   if (!ring_check(wa, slot_in >= 0 && slot_in < nring && slot_out >= 0 && slot_out < nring, 8))
     return 1;
-  unsigned long long* in_slot = pd.slots + slot_in;
-  unsigned long long* out_slot = pd.slots + slot_out;
+  double* in_bnd = has_prod ? pd.bnd + (size_t)slot_in * pd.cstride : nullptr;
+  double* out_bnd = has_cons ? pd.bnd + (size_t)slot_out * pd.cstride : nullptr;
+  unsigned long long* clr_in = has_prod ? pd.slots + (s - 1) : nullptr;   // writer s - 1's count
+  unsigned long long* clr_out = pd.slots + s;                              // this strip's count
+  unsigned long long* clr_next =                                           // the next writer's
+      has_prod && s - 1 + nring < S ? pd.slots + (s - 1 + nring) : nullptr;
   unsigned in_ok = 0, out_ok = 0;  // leading columns cleared for the input's / this strip's writer
   constexpr int kPublish = 8;      // chunks between releases of the cleared count
 
@@ -142,16 +145,11 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     if (in_ok < (unsigned)min((c + 1) << 5, C)) return kBndEmpty;
     return ld_relaxed_u64(in_bnd + col);
   };
-  // Cleared count of a slot for writer `who` (acquire: the clearing stores are visible).
-  // The word names a later writer only once the row's reader of `who`'s round has seen every
-  // column cleared for `who` (that reader publishes nothing before), so a later name means
-  // every column.
-  auto cleared = [&](unsigned long long* slot, int who, unsigned have) -> unsigned {
-    const unsigned long long w = bcast(lane == 0 ? ld_acquire(slot) : 0ull);
+  // cleared count of a writer (acquire: the clearing stores are visible)
+  auto cleared = [&](unsigned long long* cnt, unsigned have) -> unsigned {
+    const unsigned long long w = bcast(lane == 0 ? ld_acquire(cnt) : 0ull);
     __syncwarp();  // every lane's later accesses of the row are ordered after the acquire
-    const int id = (int)(unsigned)(w >> 32);
-    if (id == who) return max(have, (unsigned)w);
-    return id > who ? kSlotAll : have;
+    return max(have, (unsigned)w);
   };
   const bool store_out = has_cons && lane == 31;
 
@@ -229,7 +227,7 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     const unsigned need_in = (unsigned)min((c + 1) << 5, C);
     for (int it = 0;; ++it) {
       if (reads && in_ok < need_in) {
-        in_ok = cleared(in_slot, s - 1, in_ok);
+        in_ok = cleared(clr_in, in_ok);
         if (in_ok >= need_in) cur = load_in(c);
       }
       if (__all_sync(kFull, cur != kBndEmpty)) break;
@@ -242,17 +240,14 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     }
     if (status) break;
     if (reads) {
-      // read: the chunk's words go back to "not yet written" for the row's next writer.  The
-      // count is published only once the row's previous reader has published all of it
-      // (in_ok == kSlotAll): the slot word then passes from that reader to this one, and a
-      // later publication of that reader cannot overwrite this one's.
+      // read: the chunk's words go back to "not yet written" for the row's next writer
       const int col = (c << 5) + lane;
       if (col < C) st_relaxed_u64(reinterpret_cast<unsigned long long*>(in_bnd) + col, kBndEmpty);
-      if ((c & (kPublish - 1)) == kPublish - 1 && in_ok == kSlotAll) {
+      if ((c & (kPublish - 1)) == kPublish - 1 && clr_next) {
         __syncwarp();
         if (lane == 0) {
           __threadfence();
-          st_release(in_slot, ((unsigned long long)(unsigned)(s - 1 + nring) << 32) | need_in);
+          st_release(clr_next, need_in);
         }
       }
     }
@@ -260,7 +255,7 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
       // this chunk's steps store the last row's columns below 32c + 32 - kOutLag
       const unsigned need_out = (unsigned)min(max((c << 5) + 32 - kOutLag, 0), C);
       for (int it = 0; out_ok < need_out; ++it) {
-        out_ok = cleared(out_slot, s, out_ok);
+        out_ok = cleared(clr_out, out_ok);
         if (out_ok >= need_out) break;
         if (wt.check(it)) {
           status = 1;
@@ -277,22 +272,12 @@ __device__ int dfd_strip(const WaveArgs& wa, const PairDesc& pd, PairState* st, 
     stage(c + 1, qn);
     __syncwarp();
   }
-  if (status == 0 && has_prod) {
-    // every input word has been read and cleared: the whole row is the next writer's, once
-    // the previous reader's last publication is in (see above)
-    for (int it = 0; in_ok != kSlotAll; ++it) {
-      in_ok = cleared(in_slot, s - 1, in_ok);
-      if (in_ok != kSlotAll && wt.check(it)) {
-        status = 1;
-        break;
-      }
-    }
-  }
-  if (status == 0 && has_prod) {
+  if (status == 0 && clr_next) {
+    // every input word has been read and cleared: the whole row is the next writer's
     __syncwarp();
     if (lane == 0) {
       __threadfence();
-      st_release(in_slot, ((unsigned long long)(unsigned)(s - 1 + nring) << 32) | kSlotAll);
+      st_release(clr_next, kSlotAll);
     }
   }
   if (holds_last) st->result = res;

@@ -339,10 +339,11 @@ __global__ void dfd_fill_kernel(const PairDesc* pairs, int npairs, int rows_per_
     const long long n = rows * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
       b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
-    // ring row k is first written by strip k, every column of it cleared
+    // cleared counts: the first `ring` strips write fresh rows (every column cleared), the
+    // others wait for their row's previous reader
     if (blockIdx.x == 0)
-      for (int k = threadIdx.x; k < rows; k += blockDim.x)
-        pd.slots[k] = ((unsigned long long)k << 32) | kSlotAll;
+      for (long long k = threadIdx.x; k < S; k += blockDim.x)
+        pd.slots[k] = k < pd.ring ? kSlotAll : 0ull;
   }
 }
 
@@ -1042,7 +1043,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int64_t tstride = align_up((size_t)((tcols(p) + 31) / 32), 32);
     L.tags[p] = take(sizeof(unsigned) * L.ring_t[p] * tstride);
     L.prog[p] = take(sizeof(Prog) * std::max<int64_t>(St, (trows(p) + 31) / 32));
-    L.slots[p] = take(sizeof(unsigned long long) * std::max(L.ring_d[p], L.ring_c[p]));
+    L.slots[p] = take(sizeof(unsigned long long) * (n1s[p] + 31) / 32);  // a count per DFD strip
   }
   L.zero_end = off;
   L.active = take(sizeof(int));
