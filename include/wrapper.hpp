@@ -3,8 +3,9 @@
 // src/compute_distance_wrapper.cpp:6.  forceOversize chooses between the reference's two
 // decision paths as the reference does: forced, or when the reference's materialised interval
 // arrays would not fit in free device memory, the fused kernel's free intervals; otherwise the
-// materialised path's (they differ in one rounding, rfd.h enum rfd_formula).  The engine's
-// decision memory is O(ring rows x (n1 + n2)) either way.
+// materialised path's (they differ in one rounding, rfd.h enum rfd_formula).  Device memory is
+// the same either way: O(n1 + n2) for the curves, records and the DFD's boundary ring, plus
+// about n1 * n2 / 4 bytes of boundary rows for the VE-FD and decision strips.
 #pragma once
 
 #include "curve.hpp"
