@@ -300,6 +300,13 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
     t_c, _ = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
                                               coarse_ub=COARSE_UB), 1)
     t_p, plain = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True), 1)
+    # the same search without the network: the threshold probe over VE-FD alone (a bracket at
+    # the VE-FD bound), as a replayed graph like the learned form
+    alone = dict(precise=True, graph=True,
+                 brackets=[(r["vefd"] * (1 - 1e-15), r["vefd"]) for r in plain])
+    ctx.distance_batch(Ps, Qs, **alone)
+    t_a, thr = timed(lambda: ctx.distance_batch(Ps, Qs, **alone), 2)
+    tail = [k for k, r in enumerate(thr) if r["probes"] > 1]
     idx = list(range(0, n, max(1, n // sample)))[:sample]
     t_s, single = timed(lambda: [ctx.distance(Ps[k], Qs[k], precise=True) for k in idx], 1)
     dev = max(abs(a["distance"] - b["distance"]) / a["distance"]
@@ -316,6 +323,7 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
            "learned_batched_mixed": n / (statistics.median(t_m) * 1e-3),
            "learned_batched_coarse_ub": n / (t_c[0] * 1e-3),
            "plain_batched": n / (statistics.median(t_p) * 1e-3),
+           "threshold_only_batched": n / (statistics.median(t_a) * 1e-3),
            "plain_single_calls": len(idx) / (sum(t_s) * 1e-3)}
     return {
         "workload": "4096 uneven pairs (2D/3D 50/50, lognormal lengths median 2000, sigma 1, "
@@ -332,12 +340,60 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
         "cuda_graph": "batched forms captured once and replayed (rfd_options.graph)",
         "plain_single_sample": f"{len(idx)} pairs (every {n // len(idx)}th), one call each",
         "mean_probes": {"learned": statistics.mean(r["probes"] for r in learned),
-                        "plain": statistics.mean(r["probes"] for r in plain)},
+                        "plain": statistics.mean(r["probes"] for r in plain),
+                        "threshold_only": statistics.mean(r["probes"] for r in thr)},
+        "tail_pairs": {"count": len(tail),
+                       "mean_probes_learned": statistics.mean(learned[k]["probes"] for k in tail)
+                       if tail else None,
+                       "mean_probes_threshold_only": statistics.mean(thr[k]["probes"] for k in tail)
+                       if tail else None},
+        "bracket_network": network_timing(model, n),
         "probe_rounds": {"learned": max(r["probes"] for r in learned),
                          "plain": max(r["probes"] for r in plain)},
         "max_rel_dev_learned_vs_plain": dev,
         "cells": sum(len(p) * len(q) for p, q in pairs),
     }
+
+
+def network_timing(model, n):
+    """The bracket network's forward pass on n pairs (its hand-written mma.sync BF16 kernels)
+    against the same layer shapes on cuBLAS through torch (BF16 matmuls, FP32 accumulate, GELU),
+    CUDA events, median of 20 after 5 warm-up calls."""
+    import torch
+    x = torch.randn(n, 400, device="cuda")
+    y = torch.empty(n, 2, device="cuda")
+    w = [torch.randn(o, i, device="cuda", dtype=torch.bfloat16) * (1.0 / i ** 0.5)
+         for o, i in ((256, 400), (256, 256), (256, 256), (2, 256))]
+    xb = x.to(torch.bfloat16)
+
+    def ours():
+        model.forward(x.data_ptr(), n, y.data_ptr())
+
+    def lib():
+        h = xb
+        for k, wk in enumerate(w):
+            h = h @ wk.t()
+            if k < 3:
+                h = torch.nn.functional.gelu(h, approximate="tanh")
+        return h
+
+    def med(fn):
+        s = torch.cuda.current_stream()
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(20):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+    torch.cuda.synchronize()
+    return {"pairs": n, "ms_ours_mma_sync": med(ours), "ms_cublas_bf16_torch": med(lib),
+            "note": "the network runs once per call on its own stream; both are launch-bound"}
 
 
 def mixed_leg(ctx, model, timed, npairs):

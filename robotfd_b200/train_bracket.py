@@ -103,12 +103,20 @@ def fold(params, mu, sd, ymu, ysd):
     return p.astype(np.float32)
 
 
-def train(X, y, epochs=150, batch=512, lr=2e-3, seed=0, device=0, log=None):
+def train(X, y, epochs=150, batch=512, lr=2e-3, seed=0, device=0, log=None, val_frac=0.2,
+          patience=15):
     """Trains a fresh network on the pairs of (X, y) above the threshold; returns it with
-    the normalisations folded in, and the per-epoch loss."""
+    the normalisations folded in, and the per-epoch loss.  A fixed fifth of the pairs is held
+    out: the parameters kept are those of the epoch with the lowest held-out pinball loss, and
+    training stops after `patience` epochs without improvement (a few thousand tail pairs
+    for 234k parameters overfit otherwise, and the quantiles collapse onto each other)."""
     import torch
     ok = np.isfinite(y) & (y > THRESHOLD_Y)
     X, y = X[ok], y[ok]
+    perm0 = np.random.default_rng(seed).permutation(len(y))
+    nval = int(len(y) * val_frac)
+    Xv, yv = X[perm0[:nval]], y[perm0[:nval]]
+    X, y = X[perm0[nval:]], y[perm0[nval:]]
     mu = X.mean(0).astype(np.float64)
     sd = X.std(0).astype(np.float64)
     sd[sd < 1e-6] = 1.0
@@ -118,13 +126,16 @@ def train(X, y, epochs=150, batch=512, lr=2e-3, seed=0, device=0, log=None):
     yn = ((y - ymu) / ysd).astype(np.float32)
     dX = torch.from_numpy(Xn).to(f"cuda:{device}")
     dy = torch.from_numpy(yn).to(f"cuda:{device}")
+    dXv = torch.from_numpy(((Xv - mu) / sd).astype(np.float32)).to(f"cuda:{device}")
+    dyv = torch.from_numpy(((yv - ymu) / ysd).astype(np.float32)).to(f"cuda:{device}")
     model = rfd.Model(device, seed=seed)
     gen = torch.Generator(device=f"cuda:{device}").manual_seed(seed)
     n = len(y)
     batch = min(batch, n)
     steps_per_epoch = max(1, n // batch)
     total = epochs * steps_per_epoch
-    losses, step = [], 0
+    losses, val_losses, step = [], [], 0
+    best, best_params, since = np.inf, model.get_params(), 0
     for ep in range(epochs):
         perm = torch.randperm(n, generator=gen, device=dX.device)
         acc = 0.0
@@ -137,10 +148,40 @@ def train(X, y, epochs=150, batch=512, lr=2e-3, seed=0, device=0, log=None):
             acc += model.train_step(xb.data_ptr(), yb.data_ptr(), len(idx), cur)
             step += 1
         losses.append(acc / steps_per_epoch * ysd)
+        torch.cuda.current_stream().synchronize()
+        _, vl = model.gradients(dXv.data_ptr(), dyv.data_ptr(), len(yv)) if len(yv) else (0, 0.0)
+        val_losses.append(vl * ysd)
+        if vl < best:
+            best, best_params, since = vl, model.get_params(), 0
+        else:
+            since += 1
         if log and (ep + 1) % 10 == 0:
-            log(f"epoch {ep + 1}/{epochs}: pinball loss {losses[-1]:.4f}")
-    model.set_params(fold(model.get_params(), mu, sd, ymu, ysd))
-    return model, losses
+            log(f"epoch {ep + 1}/{epochs}: pinball loss {losses[-1]:.4f}, held out {val_losses[-1]:.4f}")
+        if since >= patience:
+            break
+    model.set_params(fold(best_params, mu, sd, ymu, ysd))
+    return model, (losses, val_losses)
+
+
+def coverage(ctx, model, Ps, Qs, plain):
+    """Per pair above the threshold: whether y lies inside the predicted [q05, q95], the
+    bracket's width and the distance of y from its middle, in decades."""
+    import torch
+    ep = np.array([r["endpoint"] for r in plain])
+    ve = np.array([r["vefd"] for r in plain])
+    y = np.array([target(r) for r in plain])
+    idx = np.nonzero(np.isfinite(y) & (y > THRESHOLD_Y) & (ve > 0))[0]
+    if len(idx) == 0:
+        return [], [], []
+    X = ctx.features([Ps[i] for i in idx], [Qs[i] for i in idx], ep[idx], ve[idx])
+    dX = torch.from_numpy(X).cuda(model.device)
+    dY = torch.empty((len(idx), 2), dtype=torch.float32, device=dX.device)
+    torch.cuda.synchronize()
+    model.forward(dX.data_ptr(), len(idx), dY.data_ptr())
+    q = dY.cpu().numpy().astype(np.float64)
+    lo, hi = np.minimum(q[:, 0], q[:, 1]), np.maximum(q[:, 0], q[:, 1])
+    yt = y[idx]
+    return (list((yt >= lo) & (yt <= hi)), list(hi - lo), list(np.abs(yt - 0.5 * (lo + hi))))
 
 
 def evaluate(ctx, model, npairs, seed, log=None):
@@ -149,6 +190,7 @@ def evaluate(ctx, model, npairs, seed, log=None):
                          "one_probe", "plain_rounds", "learned_rounds", "tol_rounds", "tail",
                          "tail_plain", "tail_learned", "tail_tol")}
     st.update(plain_s=0.0, learned_s=0.0, tol_s=0.0, max_rel_dev=0.0, max_rel_gap=0.0)
+    cover, width, resid = [], [], []
     for s in range(0, npairs, CHUNK):
         e = min(npairs, s + CHUNK)
         pairs = pairs_of(npairs, seed, s, e)
@@ -168,6 +210,10 @@ def evaluate(ctx, model, npairs, seed, log=None):
         st["plain_s"] += t1 - t0
         st["learned_s"] += t2 - t1
         st["tol_s"] += t4 - t3
+        cov = coverage(ctx, model, Ps, Qs, plain)
+        cover += cov[0]
+        width += cov[1]
+        resid += cov[2]
         st["plain_rounds"] += max(a["probes"] for a in plain)
         st["learned_rounds"] += max(b["probes"] for b in got)
         st["tol_rounds"] += max(c["probes"] for c in tol_only)
@@ -209,6 +255,9 @@ def evaluate(ctx, model, npairs, seed, log=None):
         "tail_pairs": st["tail"],
         "tail_mean_probes": {k: st["tail_" + k] / max(st["tail"], 1)
                              for k in ("plain", "learned", "tol")},
+        "tail_quantile_coverage": float(np.mean(cover)) if cover else None,
+        "tail_bracket_width_decades_median": float(np.median(width)) if width else None,
+        "tail_median_abs_error_decades": float(np.median(resid)) if resid else None,
         "max_rel_deviation_from_plain": st["max_rel_dev"],
         "max_rel_final_gap": st["max_rel_gap"],
     }
@@ -266,7 +315,9 @@ def main(argv=None):
                   "epochs": args.epochs, "lr": args.lr,
                   "mean_plain_probes": stats["mean_plain_probes"],
                   "y_quantiles_above": {q: float(np.quantile(y, q)) for q in (0.05, 0.5, 0.95)},
-                  "loss_first": losses[0], "loss_last": losses[-1]},
+                  "loss_first": losses[0][0], "loss_last": losses[0][-1],
+                  "epochs_run": len(losses[0]),
+                  "held_out_loss_best": float(min(losses[1])) if losses[1] else None},
         "eval": evaluate(ctx, model, args.eval_pairs, args.eval_seed, log),
         "out": os.path.relpath(args.out),
     }

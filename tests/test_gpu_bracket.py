@@ -7,10 +7,13 @@ from oracle import mlp_oracle
 
 pytestmark = pytest.mark.gpu
 
-# BF16 operands with FP32 accumulation against a float64 reference of the same rounded
-# operands: relative error of a whole output / gradient tensor.
-FWD_TOL = 2e-2
-GRAD_TOL = 3e-2
+# BF16 operands with FP32 accumulation against a float64 reference with the same BF16
+# rounding points: only the accumulation order and precision differ (a few 1e-7 relative per
+# dot product), which now and then moves a value across a BF16 rounding boundary (one BF16 ulp,
+# 2^-8 relative) when activations are rounded between layers.  Relative error of a whole
+# output / gradient tensor.
+FWD_TOL = 1e-3
+GRAD_TOL = 2e-3
 
 
 @pytest.fixture(scope="module")
@@ -32,7 +35,8 @@ def test_forward_matches_oracle(built, torch):
     dY = torch.empty((300, 2), dtype=torch.float32, device="cuda")
     model.forward(dX.data_ptr(), 300, dY.data_ptr())
     want, _, _ = mlp_oracle.forward(model.get_params(), X)
-    assert rel(dY.cpu().numpy(), want) < FWD_TOL
+    err = rel(dY.cpu().numpy(), want)
+    assert err < FWD_TOL, err
 
 
 @pytest.mark.parametrize("B", [37, 512])
@@ -50,7 +54,8 @@ def test_gradients_match_oracle(built, torch, B):
     o = 0
     for (n, k) in mlp_oracle.SIZES:
         for size in (n * k, n):
-            assert rel(g[o:o + size], want[o:o + size]) < GRAD_TOL, (n, k, size)
+            err = rel(g[o:o + size], want[o:o + size])
+            assert err < GRAD_TOL, (n, k, size, err)
             o += size
 
 
@@ -152,23 +157,36 @@ def test_gemm_matches_torch(built, torch, M, N, K, layout):
 
 
 def test_trained_network_saves_probes(ctx, built):
-    """The shipped network against the method without it, on held-out uneven-batch pairs."""
+    """The shipped network on held-out uneven-batch pairs (seed 4), against the plain method
+    and against the same search without the network: the threshold probe over VE-FD alone
+    (a bracket at the VE-FD bound, i.e. plain bisection above the threshold when it fails).
+    The threshold probe ends about 97 % of these pairs in one probe with or without the
+    network; the network is judged on the rest, the tail pairs, where it must save probes
+    and where its [q05, q95] must hold the true log10(FD/VEFD - 1) most of the time."""
+    import torch
     from robotfd_b200 import train_bracket
-    pairs = train_bracket.pairs_of(4096, 4, 0, 256)
+    pairs = train_bracket.pairs_of(4096, 4, 0, 4096)
     Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
     plain = ctx.distance_batch(Ps, Qs, precise=True)
     model = built.Model.pretrained(0)
-    got = ctx.distance_batch(Ps, Qs, precise=True, model=model)
+    try:
+        got = ctx.distance_batch(Ps, Qs, precise=True, model=model)
+        br = np.array([[r["vefd"] * (1 - 1e-15), r["vefd"]] for r in plain])
+        alone = ctx.distance_batch(Ps, Qs, precise=True, brackets=br)
+        cover, _, _ = train_bracket.coverage(ctx, model, Ps, Qs, plain)
+    finally:
+        model.close()
     tol = 2.0 ** -33
-    for a, b in zip(plain, got):
-        assert abs(a["distance"] - b["distance"]) <= 2 * tol * a["distance"]
-        assert b["lb"] <= b["distance"] <= b["ub"] and b["ub"] - b["lb"] <= tol * b["ub"]
+    for a, b, c in zip(plain, got, alone):
+        for r in (b, c):
+            assert abs(a["distance"] - r["distance"]) <= 2 * tol * a["distance"]
+            assert r["lb"] <= r["distance"] <= r["ub"] and r["ub"] - r["lb"] <= tol * r["ub"]
         assert b["flags"] & built.FLAG_BRACKET_USED
     mean_plain = np.mean([a["probes"] for a in plain])
-    mean_learned = np.mean([b["probes"] for b in got])
-    assert mean_learned < 0.2 * mean_plain, (mean_plain, mean_learned)
-    # pairs the threshold probe does not end: the network's bracket against plain bisection
-    tail = [k for k, b in enumerate(got) if b["probes"] > 1]
-    if tail:
-        # at most the two bracket checks more than plain bisection
-        assert np.mean([got[k]["probes"] for k in tail]) <= np.mean([plain[k]["probes"] for k in tail]) + 2
+    assert np.mean([b["probes"] for b in got]) < 0.1 * mean_plain
+    tail = [k for k, c in enumerate(alone) if c["probes"] > 1]
+    assert len(tail) > 50
+    net = np.mean([got[k]["probes"] for k in tail])
+    thr = np.mean([alone[k]["probes"] for k in tail])
+    assert net < thr - 0.5, (net, thr)             # measured saving on the tail
+    assert np.mean(cover) > 0.6, np.mean(cover)    # calibrated quantiles (held-out tail pairs)
