@@ -283,8 +283,12 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
             "mean_probes": {"learned": statistics.mean(r["probes"] for r in res)},
         }
     import robotfd_b200 as rfd
-    # the project's autotuner picks the DFD sweep's tile shape for this workload
+    # the project's autotuners pick the DFD sweep's tile shape and the team strips' shape and
+    # search split for this workload (the learned form, on a sample of the batch)
     tuned = ctx.autotune(Ps, Qs, reps=1)
+    samp = list(range(0, n, 4))
+    tuned_search = ctx.autotune_search([Ps[k] for k in samp], [Qs[k] for k in samp], reps=1,
+                                       precise=True, model=model)
     ctx.distance_batch(Ps[:64], Qs[:64], precise=True, model=model)  # warm
     # the batched forms run as CUDA graphs: the first (untimed) call captures, the timed
     # calls with the same layout replay
@@ -336,7 +340,13 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
         "mixed": {"max_rel_error_vs_fp64": mixed_err, "decision_cells_fp64_fraction": fp64_frac},
         "autotune": {"dfd_rows_per_lane": tuned["rows"], "dfd_skewed": tuned["skew"],
                      "ms": {f"{r}x{'skew' if k else 'stack'}": round(v, 2)
-                            for (r, k), v in tuned["ms"].items()}},
+                            for (r, k), v in tuned["ms"].items()},
+                     "team_warps": tuned_search["warps"],
+                     "search_switch": tuned_search["switch"],
+                     "search_window": tuned_search["window"],
+                     "search_sample": f"{len(samp)} pairs (every 4th), learned form",
+                     "search_ms": {f"w{w}_s{['quarter', 'teams', 'queue'][si]}_win{win}":
+                                   round(v, 2) for (w, si, win), v in tuned_search["ms"].items()}},
         "cuda_graph": "batched forms captured once and replayed (rfd_options.graph)",
         "plain_single_sample": f"{len(idx)} pairs (every {n // len(idx)}th), one call each",
         "mean_probes": {"learned": statistics.mean(r["probes"] for r in learned),

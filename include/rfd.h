@@ -195,6 +195,21 @@ int32_t rfd_autotune(rfd_context* ctx, int64_t npairs, const double* const* c1s,
                      const double* const* c2s, const int64_t* n2s, const int32_t* dims,
                      const rfd_options* opt, int32_t reps, double* ms_out, int32_t* best_out);
 
+/* Autotuner of the team strips' shape and of the batched search's split (no reference
+   counterpart: the reference fixes its launch shape).  Times every combination of warps per
+   team (4 or 8), the switch point from probe rounds run as launches to the continuous queue
+   (a quarter of the team count of active pairs, the team count, or the queue from the first
+   probe: INT32_MAX) and the continuous search's start window (1, 2 or 4
+   strips), on whole solves of the caller's pairs with the caller's options (`reps` timed calls
+   each, after one untimed one), and keeps the fastest in the context for later calls.
+   ms_out (optional): 18 doubles, ms per solve at [(warps index * 3 + switch index) * 3 +
+   window index].  best_out (optional): 3 ints, warps per team, switch point, window kept.
+   The strip height is the warp width (32 rows, a lane per row) and is not tuned. */
+int32_t rfd_autotune_search(rfd_context* ctx, int64_t npairs, const double* const* c1s,
+                            const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
+                            const int32_t* dims, const rfd_options* opt, int32_t reps,
+                            double* ms_out, int32_t* best_out);
+
 /* All pairwise distances of ncurves curves (no reference counterpart: the many-to-many use of
    the reference's Curves, include/curve.hpp:42-47).  out is ncurves x ncurves, row-major,
    symmetric with a zero diagonal; entry (i, j), i < j, is the distance with curve i as the

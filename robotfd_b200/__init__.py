@@ -61,7 +61,7 @@ EXPORTS = (
     "rfd_model_num_params", "rfd_model_create", "rfd_model_destroy", "rfd_model_set_params",
     "rfd_model_get_params", "rfd_model_forward", "rfd_model_gradients", "rfd_model_train_step",
     "rfd_features", "rfd_gemm_bf16", "rfd_interval_class", "rfd_distance_matrix",
-    "rfd_load_txt_fast", "rfd_save_bin", "rfd_load_bin", "rfd_autotune",
+    "rfd_load_txt_fast", "rfd_save_bin", "rfd_load_bin", "rfd_autotune", "rfd_autotune_search",
 )
 
 
@@ -182,6 +182,8 @@ def lib():
     L.rfd_distance_matrix.restype = i32
     L.rfd_autotune.argtypes = [vp, i64, vp, _i64p, vp, _i64p, _i32p, vp, i32, _dp, _i32p]
     L.rfd_autotune.restype = i32
+    L.rfd_autotune_search.argtypes = [vp, i64, vp, _i64p, vp, _i64p, _i32p, vp, i32, _dp, _i32p]
+    L.rfd_autotune_search.restype = i32
     L.rfd_decide_noalloc.argtypes = [vp, i64, vp, i64, i32, dbl, vp, vp]
     L.rfd_decide_noalloc.restype = i32
     fp = ctypes.POINTER(ctypes.c_float)
@@ -372,6 +374,33 @@ class Context:
         return {"rows": int(best[0]), "skew": int(best[1]),
                 "ms": {(r, k): float(ms[i * 2 + k]) for i, r in enumerate((1, 2, 4, 8))
                        for k in (0, 1)}}
+
+    def autotune_search(self, Ps, Qs, reps=1, **kw):
+        """Times the team strips' shape (4 or 8 warps) and the search's split (switch point,
+        start window) on whole solves of these pairs with these options, and keeps the fastest
+        in the context (rfd_autotune_search).  Returns {"warps", "switch", "window", "ms":
+        {(warps, switch index, window): ms per solve}}."""
+        n = len(Ps)
+        if n != len(Qs) or n == 0:
+            raise ValueError("Ps and Qs: non-empty, same length")
+        A = [_curve(p) for p in Ps]
+        B = [_curve(q) for q in Qs]
+        p1 = (ctypes.c_void_p * n)(*[a.ctypes.data for a in A])
+        p2 = (ctypes.c_void_p * n)(*[b.ctypes.data for b in B])
+        n1 = np.array([len(a) for a in A], dtype=np.int64)
+        n2 = np.array([len(b) for b in B], dtype=np.int64)
+        dm = np.array([a.shape[1] for a in A], dtype=np.int32)
+        o = options(**kw)
+        ms = np.zeros(18)
+        best = np.zeros(3, dtype=np.int32)
+        _check(lib().rfd_autotune_search(self._h, n, p1, n1.ctypes.data_as(_i64p), p2,
+                                         n2.ctypes.data_as(_i64p), dm.ctypes.data_as(_i32p),
+                                         ctypes.byref(o), int(reps), ms.ctypes.data_as(_dp),
+                                         best.ctypes.data_as(_i32p)))
+        return {"warps": int(best[0]), "switch": int(best[1]), "window": int(best[2]),
+                "ms": {(w, si, win): float(ms[(wi * 3 + si) * 3 + ni])
+                       for wi, w in enumerate((4, 8)) for si in range(3)
+                       for ni, win in enumerate((1, 2, 4))}}
 
     def distance_matrix(self, curves, budget_bytes=0.0, with_results=False, **kw):
         """All pairwise distances (rfd_distance_matrix): an (n, n) array, symmetric, zero

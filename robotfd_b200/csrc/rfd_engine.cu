@@ -473,8 +473,9 @@ __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, i
 // teams.  The CTA whose strip ends a pair's probe clears the boundary words the probe's
 // strips wrote (each strip records its written chunk range), then starts the next probe: a
 // pair starts its next probe as soon as its last one ends, not after every pair's.
-template <int KIND>
-__global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
+template <int KIND, int NW = kTeamThreads / 32>
+__global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
+  constexpr int H = NW - 1;  // helper warps
   extern __shared__ __align__(128) unsigned char team_smem[];
   TeamShared* sh = (TeamShared*)team_smem;
   double2* tiles = (double2*)(team_smem + kTeamHeader);
@@ -482,10 +483,10 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int k = 0; k < 2; ++k) {
-      mbar_init(&sh->full[k], kHelpers);
+      mbar_init(&sh->full[k], H);
       mbar_init(&sh->req[k], 1);
     }
-    mbar_init(&sh->staged, kHelpers);
+    mbar_init(&sh->staged, H);
   }
   __syncthreads();
   unsigned seqP = 0, seqC = 0, seqH = 0, seqS = 0;
@@ -535,8 +536,8 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
                                    : team_propagator<KIND, 3>(wa, pd, st, s, sh, tiles, seqP, seqC);
       if (lane == 0) sh->status = status;
     } else {
-      if (pd.d == 2) team_helpers<KIND, 2>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
-      else team_helpers<KIND, 3>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
+      if (pd.d == 2) team_helpers<KIND, 2, H>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
+      else team_helpers<KIND, 3, H>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
     }
     __syncthreads();
     const int S = (pd.n1 - 1 + 31) >> 5;
@@ -565,7 +566,7 @@ __global__ void __launch_bounds__(kTeamThreads) team_kernel(WaveArgs wa) {
     if (KIND == K_DEC && sh->push) {
       // the probe's written boundary words back to "not yet written", one strip per warp
       const long long C = pd.n2 - 1;
-      for (int r = warp; r < S - 1; r += kTeamThreads / 32) {
+      for (int r = warp; r < S - 1; r += NW) {
         const int lo = pd.prog[r].wlo, hi = pd.prog[r].whi;
         double* row = pd.bnd + (size_t)r * pd.cstride;
         const long long end = min((long long)(hi + 1) << 5, C);
@@ -710,7 +711,9 @@ struct rfd_context {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   int grid[3] = {0, 0, 0};
-  int team_grid[3] = {0, 0, 0};
+  int team_grid[3] = {0, 0, 0};     // teams of the chosen shape (team_warps)
+  int team_grids[2][3] = {{0, 0, 0}, {0, 0, 0}};  // [teams of 4, of 8 warps][kind]
+  int team_warps = 8;  // warps per team: 8 or 4 (RFD_TEAM_WARPS, rfd_autotune_search)
   int solo = 0;  // RFD_SOLO=1: VE-FD and decisions on the solo-warp strips (A/B checks)
   int lockstep = 0;  // RFD_LOCKSTEP=1: one launch per probe round instead of the continuous search
   int search_switch = 0;  // active pairs below which the continuous search takes over
@@ -744,6 +747,15 @@ struct rfd_context {
 namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// The team kernel of the context's shape (warps per team) on its grid.
+template <int KIND>
+void launch_team(const rfd_context* ctx, const WaveArgs& wa, cudaStream_t st) {
+  if (ctx->team_warps == 4)
+    team_kernel<KIND, 4><<<ctx->team_grid[KIND], 128, team_smem_bytes<KIND>(), st>>>(wa);
+  else
+    team_kernel<KIND, 8><<<ctx->team_grid[KIND], 256, team_smem_bytes<KIND>(), st>>>(wa);
+}
 
 int ring_of(int64_t strips, int rows) {  // strips - 1 rows are handed over; at least 1
   return (int)std::max<int64_t>(1, std::min<int64_t>(strips - 1, rows));
@@ -1396,7 +1408,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
           wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
         } else {
           fill(ph);
-          team_kernel<K_VEFD><<<ctx->team_grid[K_VEFD], kTeamThreads, team_smem_bytes<K_VEFD>(), st>>>(wa);
+          launch_team<K_VEFD>(ctx, wa, st);
         }
         RFD_CUDA(cudaGetLastError());
       }
@@ -1430,7 +1442,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         wa.gate = (int*)(counters + L.nlaunch + k);
         wa.gate_min = ctx->search_switch;
         fill(PH_SEARCH);
-        team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+        launch_team<K_DEC>(ctx, wa, st);
         RFD_CUDA(cudaGetLastError());
         ++launches;
       }
@@ -1449,7 +1461,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       fill(PH_SEARCH);
       search_queue_init_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
           dt, ds, (int)npairs, wa);
-      team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+      launch_team<K_DEC>(ctx, wa, st);
       RFD_CUDA(cudaGetLastError());
       launches += 2;
       wa.nitems = nstatic;
@@ -1464,7 +1476,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
       } else {
         fill(PH_SEARCH);
-        team_kernel<K_DEC><<<ctx->team_grid[K_DEC], kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+        launch_team<K_DEC>(ctx, wa, st);
       }
       RFD_CUDA(cudaGetLastError());
       ++launches;
@@ -1486,7 +1498,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     const int flags[] = {mode, (int)on_device, (int)drop, ck, max_probes, o.stop_mode, o.reference_quirks,
                          o.dense, o.precision, o.bracket != nullptr, ctx->timing, ctx->prof,
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
-                         ctx->search_switch, ctx->search_window, (int)(ctx->spin_cycles >> 32),
+                         ctx->search_switch, ctx->search_window, ctx->team_warps,
+                         (int)(ctx->spin_cycles >> 32),
                          (int)(ctx->spin_cycles & 0xffffffff)};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
@@ -1672,18 +1685,29 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
   for (int k = 0; k < 3; ++k) c->grid[k] = std::max(1, occ[k]) * c->num_sms;
   {
     const size_t sm_ve = team_smem_bytes<K_VEFD>(), sm_dec = team_smem_bytes<K_DEC>();
-    if (cudaFuncSetAttribute(team_kernel<K_VEFD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(team_kernel<K_VEFD, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm_ve) != cudaSuccess ||
-        cudaFuncSetAttribute(team_kernel<K_DEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(team_kernel<K_DEC, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm_dec) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_VEFD, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm_ve) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_DEC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm_dec) != cudaSuccess) {
       delete c;
       return fail(RFD_ERR_CUDA, "cudaFuncSetAttribute(team smem)");
     }
-    int o1 = 0, o2 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, team_kernel<K_VEFD>, kTeamThreads, sm_ve);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, team_kernel<K_DEC>, kTeamThreads, sm_dec);
-    c->team_grid[K_VEFD] = std::max(1, o1) * c->num_sms;
-    c->team_grid[K_DEC] = std::max(1, o2) * c->num_sms;
+    int o[4] = {0, 0, 0, 0};
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], team_kernel<K_VEFD, 4>, 128, sm_ve);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], team_kernel<K_DEC, 4>, 128, sm_dec);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], team_kernel<K_VEFD, 8>, 256, sm_ve);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], team_kernel<K_DEC, 8>, 256, sm_dec);
+    c->team_grids[0][K_VEFD] = std::max(1, o[0]) * c->num_sms;
+    c->team_grids[0][K_DEC] = std::max(1, o[1]) * c->num_sms;
+    c->team_grids[1][K_VEFD] = std::max(1, o[2]) * c->num_sms;
+    c->team_grids[1][K_DEC] = std::max(1, o[3]) * c->num_sms;
+    const char* tw = getenv("RFD_TEAM_WARPS");
+    c->team_warps = tw && tw[0] == '4' && !tw[1] ? 4 : 8;
+    for (int k = 0; k < 3; ++k) c->team_grid[k] = c->team_grids[c->team_warps == 4 ? 0 : 1][k];
     const char* e = getenv("RFD_SOLO");
     c->solo = e && e[0] == '1';
     const char* ls = getenv("RFD_LOCKSTEP");
@@ -1921,6 +1945,68 @@ int32_t rfd_autotune(rfd_context* ctx, int64_t npairs, const double* const* c1s,
   if (best_out) {
     best_out[0] = ctx->dfd_rows;
     best_out[1] = ctx->dfd_skew;
+  }
+  return rc;
+}
+
+// Autotuner of the team strips' shape and of the search's split between probe rounds run as
+// launches and the continuous queue: warps per team (4: 3 helpers, twice the teams; 8: 7
+// helpers), the switch point (active pairs below which the continuous search takes over: a
+// quarter of the team count, the team count, or every pair from the first probe) and the start window (strips a probe queues ahead: 1, 2,
+// 4).  Each candidate solves the caller's pairs once untimed and `reps` times timed (CUDA-event
+// phase times of whole solves with the caller's options); the fastest is kept in the context.
+int32_t rfd_autotune_search(rfd_context* ctx, int64_t npairs, const double* const* c1s,
+                            const int64_t* n1s, const double* const* c2s, const int64_t* n2s,
+                            const int32_t* dims, const rfd_options* opt, int32_t reps,
+                            double* ms_out, int32_t* best_out) {
+  if (!ctx || npairs < 1 || reps < 1 || reps > 100) return fail(RFD_ERR_ARG, "autotune arguments");
+  RFD_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->ev[0])
+    for (int k = 0; k < 4; ++k) RFD_CUDA(cudaEventCreate(&ctx->ev[k]));
+  rfd_options o;
+  rfd_options_init(&o, 1);
+  if (opt) o = *opt;
+  o.graph = 0;
+  const int keep_w = ctx->team_warps, keep_sw = ctx->search_switch, keep_win = ctx->search_window,
+            keep_timing = ctx->timing;
+  double keep_acc[7];
+  memcpy(keep_acc, ctx->acc, sizeof(keep_acc));
+  std::vector<rfd_result> res((size_t)npairs);
+  const int warps[2] = {4, 8}, windows[3] = {1, 2, 4};
+  double best = 1e300;
+  int bw = keep_w, bs = keep_sw, bn = keep_win, rc = RFD_OK;
+  for (int wi = 0; wi < 2 && rc == RFD_OK; ++wi)
+    for (int si = 0; si < 3 && rc == RFD_OK; ++si)
+      for (int ni = 0; ni < 3 && rc == RFD_OK; ++ni) {
+        ctx->team_warps = warps[wi];
+        for (int k = 0; k < 3; ++k) ctx->team_grid[k] = ctx->team_grids[wi][k];
+        ctx->search_switch = si == 0 ? ctx->team_grid[K_DEC] / 4
+                             : si == 1 ? ctx->team_grid[K_DEC] : INT32_MAX;
+        ctx->search_window = windows[ni];
+        ctx->timing = 1;
+        rc = run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, &o, res.data(), MODE_DISTANCE, 0.0);
+        for (int k = 0; k < 7; ++k) ctx->acc[k] = 0;
+        for (int r = 0; r < reps && rc == RFD_OK; ++r)
+          rc = run_batch(ctx, npairs, c1s, n1s, c2s, n2s, dims, &o, res.data(), MODE_DISTANCE, 0.0);
+        const double ms = rc == RFD_OK ? (ctx->acc[0] + ctx->acc[1] + ctx->acc[2]) / reps : -1.0;
+        if (ms_out) ms_out[(wi * 3 + si) * 3 + ni] = ms;
+        if (rc == RFD_OK && ms < best) {
+          best = ms;
+          bw = warps[wi];
+          bs = ctx->search_switch;
+          bn = windows[ni];
+        }
+      }
+  ctx->team_warps = rc == RFD_OK ? bw : keep_w;
+  for (int k = 0; k < 3; ++k) ctx->team_grid[k] = ctx->team_grids[ctx->team_warps == 4 ? 0 : 1][k];
+  ctx->search_switch = rc == RFD_OK ? bs : keep_sw;
+  ctx->search_window = rc == RFD_OK ? bn : keep_win;
+  ctx->timing = keep_timing;
+  memcpy(ctx->acc, keep_acc, sizeof(keep_acc));
+  if (best_out) {
+    best_out[0] = ctx->team_warps;
+    best_out[1] = ctx->search_switch;
+    best_out[2] = ctx->search_window;
   }
   return rc;
 }
@@ -2194,10 +2280,10 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
       void* p = nullptr;
       RFD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
       const size_t sm_dec = team_smem_bytes<K_DEC>();
-      RFD_CUDA(cudaFuncSetAttribute(team_kernel<K_DEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      RFD_CUDA(cudaFuncSetAttribute(team_kernel<K_DEC, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sm_dec));
       int occ = 0, nsm = 0, clk = 0;
-      RFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, team_kernel<K_DEC>, kTeamThreads,
+      RFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, team_kernel<K_DEC, 8>, kTeamThreads,
                                                              sm_dec));
       RFD_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
       RFD_CUDA(cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, dev));
@@ -2271,7 +2357,7 @@ extern "C" int32_t rfd_decide_noalloc(const double* c1, int64_t n1, const double
   wa.active_pairs = (int*)(base + o_active);
   wa.spin_cycles = env_spin_cycles(nd.spin_cycles);
   wa.prof = nullptr;
-  team_kernel<K_DEC><<<nd.team_grid, kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
+  team_kernel<K_DEC, 8><<<nd.team_grid, kTeamThreads, team_smem_bytes<K_DEC>(), st>>>(wa);
   RFD_CUDA(cudaGetLastError());
   noalloc_emit_kernel<<<1, 32, 0, st>>>(dstate, wa.error, right_ub);
   RFD_CUDA(cudaGetLastError());

@@ -21,12 +21,13 @@
 
 namespace rfd {
 
+// Warps per team: 8 by default (warp 0 propagates, 7 helpers); teams of 4 (3 helpers) are the
+// autotuner's other shape (rfd_autotune_search), twice as many teams of half the tile rate.
 constexpr int kTeamThreads = 256;
-constexpr int kHelpers = kTeamThreads / 32 - 1;  // helper warps per team
 constexpr int kStop = -2;  // request word: strip finished
 
 struct TeamShared {
-  unsigned long long full[2];  // helpers -> propagator: tile ready (kHelpers arrivals)
+  unsigned long long full[2];  // helpers -> propagator: tile ready (one arrival per helper)
   unsigned long long req[2];   // propagator -> helpers: chunk requested (1 arrival)
   unsigned long long staged;   // helpers -> helpers: a tile's column records are staged
   int req_chunk[2];
@@ -122,7 +123,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
 
 // ------------------------------------------------------------------ helpers (warps 1..3)
 
-template <int KIND, int D>
+template <int KIND, int D, int H /* helper warps */>
 __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairState* st, int s,
                              TeamShared* sh, double2* tiles, double* stage, unsigned& seqH,
                              unsigned& seqS, int hw) {
@@ -162,13 +163,13 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     {
       const int base = (c << 5) - 31;
       const int t = (hw << 5) + lane;
-      for (int e = t; e < kStageRow * D; e += 32 * kHelpers) {
+      for (int e = t; e < kStageRow * D; e += 32 * H) {
         const int jj = e / D, k = e - jj * D;
         const int qi = min(max(base + jj, 0), C);
         buf[k * kStageRow + jj] = __ldg(pd.Q + (size_t)qi * D + k);
       }
       constexpr int W = RecW<D>::value;
-      for (int e = t; e < kStageRow - 1; e += 32 * kHelpers) {
+      for (int e = t; e < kStageRow - 1; e += 32 * H) {
         const int j = min(max(base + e, 0), C - 1);
         const double2 a = __ldg(pd.colrec + (size_t)j * W + (W - 1));
         buf[3 * kStageRow + e] = a.x;
@@ -190,7 +191,7 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
       col.A = buf[3 * kStageRow + jj];
       col.inv2A = buf[4 * kStageRow + jj];
     };
-    // Two independent cells (u, u + kHelpers) per iteration; results are stored only for
+    // Two independent cells (u, u + H) per iteration; results are stored only for
     // cells inside the grid.
     auto one = [&](int u, const ColRec<KIND, D>& col) {
       const int j = (c << 5) + u - lane;
@@ -231,9 +232,9 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
       }
       count += ok ? 1 : 0;
     };
-    for (int u0 = hw; u0 < 32; u0 += 2 * kHelpers) {
+    for (int u0 = hw; u0 < 32; u0 += 2 * H) {
       if (__shfl_sync(kFull, *(volatile int*)&sh->cancel[slot], 0)) break;
-      const int u1 = u0 + kHelpers;
+      const int u1 = u0 + H;
       ColRec<KIND, D> c0, c1;
       col_at(u0, c0);
       col_at(min(u1, 31), c1);
