@@ -1040,7 +1040,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * (L.nlaunch + max_probes + 1));
-  const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + 3 * kTrace));
+  const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + kTraceW * kTrace));
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {
     // boundary rows: team strips of 32 segment rows, one row each; the DFD ring for strips of
@@ -1550,7 +1550,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                                       " failed (boundary ring index out of range)");
   if (hmisc[1]) return fail(RFD_ERR_TIMEOUT, "an inter-warp wait exceeded its budget");
   if (ctx->prof) {
-    std::vector<unsigned long long> pc(kTraceBase + 3 * kTrace);
+    std::vector<unsigned long long> pc(kTraceBase + kTraceW * kTrace);
     RFD_CUDA(cudaMemcpy(pc.data(), dbase + prof_off, sizeof(unsigned long long) * pc.size(),
                         cudaMemcpyDeviceToHost));
     fprintf(stderr,
@@ -1561,14 +1561,23 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
             pc[8] / 1e6, pc[9] / 1e6, pc[10], pc[11] / 1e6, pc[12]);
     // strip chain of the first pair: handoff = first live input of strip s after the first
     // live output of strip s-1; lag = first live output of strip s after its first live input
-    std::vector<double> hand, lag, adv;
+    // (lag split: input -> its tile taken -> its steps done -> the next chunk's input in hand
+    // -> the first live output flushed)
+    std::vector<double> hand, lag, adv, l1, l2, l3, l4;
     const unsigned long long* tr = pc.data() + kTraceBase;
     for (int s = 1; s < kTrace; ++s) {
-      const unsigned long long in = tr[3 * s + 1], out = tr[3 * s + 2], pout = tr[3 * (s - 1) + 2];
+      const unsigned long long* t = tr + kTraceW * s;
+      const unsigned long long in = t[1], out = t[2], pout = tr[kTraceW * (s - 1) + 2];
       if (!in || !out || !pout) continue;
       hand.push_back((double)in - (double)pout);
       lag.push_back((double)out - (double)in);
       adv.push_back((double)out - (double)pout);
+      if (t[3] && t[4] && t[5]) {
+        l1.push_back((double)t[3] - (double)in);
+        l2.push_back((double)t[4] - (double)t[3]);
+        l3.push_back((double)t[5] - (double)t[4]);
+        l4.push_back((double)out - (double)t[5]);
+      }
     }
     auto med = [](std::vector<double> v) {
       if (v.empty()) return 0.0;
@@ -1577,6 +1586,9 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     };
     fprintf(stderr, "rfd trace (ns, median over %zu strips): handoff %.0f  lag %.0f  advance %.0f\n",
             hand.size(), med(hand), med(lag), med(adv));
+    fprintf(stderr, "rfd trace lag split (ns, %zu strips): input->tile %.0f  tile->steps %.0f  "
+            "steps->next input %.0f  next input->output %.0f\n",
+            l1.size(), med(l1), med(l2), med(l3), med(l4));
   }
   if (ctx->timing) {
     float a = 0.f, b = 0.f, c = 0.f;

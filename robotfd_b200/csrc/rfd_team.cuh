@@ -268,8 +268,10 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
 // ------------------------------------------------------------------ propagator (warp 0)
 
 // RFD_PROF trace of the first kTrace strips of the first pair: wall-clock ns (globaltimer,
-// comparable across SMs) at strip start, first live input chunk, first live output flush.
+// comparable across SMs) at strip start, first live input chunk, first live output flush, the
+// first live chunk's tile taken, its steps done, and the next chunk's input in hand.
 constexpr int kTrace = 512;
+constexpr int kTraceW = 6;  // trace words per strip
 constexpr int kTraceBase = 16;
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -305,8 +307,9 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   const long long t0 = clock64();
   if (wa.prof && lane == 0) atomicAdd(&wa.prof[7], 1ull);
   unsigned long long* trace =
-      (wa.prof && st == wa.st && s < kTrace) ? wa.prof + kTraceBase + 3 * s : nullptr;
+      (wa.prof && st == wa.st && s < kTrace) ? wa.prof + kTraceBase + kTraceW * s : nullptr;
   bool traced_in = false;
+  int trace_step = 0;  // 1: first live chunk's tile taken, 2: its steps done, 3: next input in
   if (trace && lane == 0) trace[0] = global_ns();
 
   const int i = (s << 5) + lane;
@@ -498,6 +501,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       // lower bound, so no release is needed.
       if (has_cons && lane == 0 && first_live_out == kNone) out_prog->first_live = (unsigned)c;
     }
+    if (trace && trace_step == 2) {
+      trace_step = 3;
+      if (lane == 0) trace[5] = global_ns();
+    }
     if (trace && in_live && !traced_in) {
       traced_in = true;
       if (lane == 0) trace[1] = global_ns();
@@ -606,6 +613,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     }
     const int slot = take();
     if (slot < 0) { status = 1; break; }
+    if (trace && traced_in && trace_step == 0) {
+      trace_step = 1;
+      if (lane == 0) trace[3] = global_ns();
+    }
     pending = -1;
     if (((c + 1) << 5) < nsteps) {  // speculative: the next chunk is usually processed too
       request(c + 1);
@@ -665,6 +676,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     if (wa.prof && lane == 0) {
       atomicAdd(&wa.prof[3], (unsigned long long)(clock64() - ts0));
       atomicAdd(&wa.prof[5], 1ull);
+    }
+    if (trace && trace_step == 1) {
+      trace_step = 2;
+      if (lane == 0) trace[4] = global_ns();
     }
     // the next chunk's input words load while this chunk is flushed and the next one set up;
     // issued before the steps, the load slowed every step by about a third
