@@ -18,18 +18,21 @@
  *                                 (src/compute_distance_wrapper.cpp:6); VE-FD launch rule .cu:1343
  *
  * Arithmetic contract (shared bit for bit with the CUDA kernels): FP64, compiled with
- * -ffp-contract=off; every "acc += x*y" of the reference is fma(x, y, acc) starting from
- * acc = 0.0 (or -r^2), "b*b - 4*A*C" is fma(b, b, -((4*A)*C)), q = t*ab + a is
- * fma(t, ab, a); sqrt and '/' are IEEE correctly rounded on both sides.  The endpoint
+ * -ffp-contract=off, restating the reference kernels as nvcc compiles them (default
+ * contraction): a sum of squares from 0.0 is sq_sum() (the zero start folds away and the
+ * first square is fused with the second); every other "acc += x*y" is fma(x, y, acc)
+ * starting from acc = 0.0 (or -r^2); "b*b - 4*A*C" is fma(b, b, -((4*A)*C)); q = t*ab + a
+ * is fma(t, ab, a); sqrt and '/' are IEEE correctly rounded on both sides.  The endpoint
  * bound and the bisection midpoint are host arithmetic in the reference (g++, no FMA) and
  * are restated without fusion.
  *
  * Parity pin: the reference has no tests or golden data.  The search driver, stop rule,
  * endpoint bound and loaders are pinned by the reference's own host code run on the same
  * inputs (tests/golden/reference_host.json, made through oracle/refharness/); the DFD,
- * VE-FD and decision cells by mathematical known-answer tests and independent
- * brute-force definitions (tests/test_oracle.py).  They are not pinned to outputs of the
- * reference's GPU kernels, which are not run here.
+ * VE-FD and decision cells by the reference's own GPU kernels run once on a B200 on four
+ * seeded pairs (tests/golden/reference_gpu.json: bounds, every probe and its decision),
+ * by mathematical known-answer tests and by independent brute-force definitions
+ * (tests/test_oracle.py).
  */
 #include <float.h>
 #include <math.h>
@@ -70,14 +73,26 @@ typedef struct {
   int mat;               /* decision: the materialised path's rounding of C (see free_interval) */
 } ora_t;
 
-/* |a-b|^2 by an fma chain from 0.0 (DFD .cu:615-619). */
-static inline double dist_sq_fma(const double* a, const double* b, int d) {
-  double s = 0.0;
-  for (int k = 0; k < d; ++k) {
-    double t = a[k] - b[k];
-    s = fma(t, t, s);
-  }
+/* Sum of squares t_0^2 + ... + t_{d-1}^2 as nvcc compiles the reference's
+   "s = 0.0; for k: s += t_k * t_k" loops (DFD .cu:615-619, segment lengths .cu:1004-1007 and
+   :1133-1137, VE-FD .cu:381-392): the zero start folds away (a square is never -0), the
+   first product is fused with the second one rounded, fma(t0, t0, t1*t1), and each later
+   square is fused into the running sum, fma(t2, t2, s).  Pinned by the reference's own
+   GPU output (tests/golden/reference_gpu.json: a 2D DFD that the source-order chain
+   fma(t1, t1, t0*t0) misses by one ulp). */
+static inline double sq_sum(const double* t, int d) {
+  if (d == 1) return t[0] * t[0];
+  double s = t[1] * t[1];
+  s = fma(t[0], t[0], s);
+  for (int k = 2; k < d; ++k) s = fma(t[k], t[k], s);
   return s;
+}
+
+/* |a-b|^2 (DFD .cu:615-619). */
+static inline double dist_sq_fma(const double* a, const double* b, int d) {
+  double t[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < d; ++k) t[k] = a[k] - b[k];
+  return sq_sum(t, d);
 }
 
 /* |a-b|^2 without fusion (host Point::dist_sqr). */
@@ -102,13 +117,12 @@ static inline double pt_seg_sq(const double* x, const double* a, const double* b
   }
   double t = apab / ab2;
   t = cmin(1.0, cmax(0.0, t));
-  double w = 0.0;
+  double dd[3] = {0.0, 0.0, 0.0};
   for (int k = 0; k < d; ++k) {
     double q = fma(t, b[k] - a[k], a[k]);
-    double dd = x[k] - q;
-    w = fma(dd, dd, w);
+    dd[k] = x[k] - q;
   }
-  return w;
+  return sq_sum(dd, d);
 }
 
 /* Free interval of segment a -> b inside the ball of radius^2 r2 around x (.cu:1175-1199):
@@ -117,14 +131,14 @@ static inline double pt_seg_sq(const double* x, const double* a, const double* b
    of mi^2 from 0, then minus r2 (mm - radius2), one rounding more than the fused chain. */
 static inline void free_interval(const double* x, const double* a, const double* b, double A,
                                  double inv2A, double r2, int d, int mat, double* lo, double* hi) {
-  double B = 0.0, Cc = mat ? 0.0 : -r2;
+  double B = 0.0, Cc = -r2, m[3] = {0.0, 0.0, 0.0};
   for (int k = 0; k < d; ++k) {
     double di = b[k] - a[k];
-    double mi = a[k] - x[k];
-    B = fma(mi, di, B);
-    Cc = fma(mi, mi, Cc);
+    m[k] = a[k] - x[k];
+    B = fma(m[k], di, B);
+    Cc = fma(m[k], m[k], Cc);
   }
-  if (mat) Cc = Cc - r2;
+  if (mat) Cc = sq_sum(m, d) - r2;
   B = B * 2.0;
   double disc = fma(B, B, -((4.0 * A) * Cc));
   *lo = -1.0;
@@ -244,11 +258,9 @@ static int prep_segments(const double* X, int64_t n, int d, double** A, double**
   *inv = (double*)malloc(sizeof(double) * (m > 0 ? m : 1));
   if (!*A || !*inv) return -1;
   for (int64_t i = 0; i < m; ++i) {
-    double s = 0.0;
-    for (int k = 0; k < d; ++k) {
-      double t = X[(i + 1) * d + k] - X[i * d + k];
-      s = fma(t, t, s);
-    }
+    double t[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < d; ++k) t[k] = X[(i + 1) * d + k] - X[i * d + k];
+    double s = sq_sum(t, d);
     (*A)[i] = s;
     (*inv)[i] = 0.5 / s;
   }
@@ -267,7 +279,7 @@ static int run_mat(int kind, const double* P, int64_t n1, const double* Q, int64
   o.seed = seed;
   o.R = kind == K_DFD ? n1 : n1 - 1;
   o.C = kind == K_DFD ? n2 : n2 - 1;
-  if (o.R < 1 || o.C < 1) return -1;
+  if (o.R < 1 || o.C < 1 || d < 1 || d > 3) return -1;
   if (kind != K_DFD) {
     if (prep_segments(P, n1, d, &o.rowA, &o.rowInv) || prep_segments(Q, n2, d, &o.colA, &o.colInv))
       return -2;

@@ -171,16 +171,28 @@ __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned l
 // ------------------------------------------------------------------ cell arithmetic
 // Every operation is an explicit round-to-nearest intrinsic, so the result does not
 // depend on the compiler's contraction choices; the CPU oracle performs the same ops.
+// They restate the reference kernels as nvcc compiles them with its default contraction.
+
+// Sum of squares of t[0..D): the reference's "s = 0.0; s += t*t" loops (DFD .cu:615-619,
+// segment lengths .cu:1004-1007 and :1133-1137, VE-FD .cu:381-392) compile with the zero
+// start folded away and the first square fused with the second one rounded,
+// fma(t0, t0, t1*t1); each later square is fused into the running sum.  (The source-order
+// chain fma(t1, t1, t0*t0) misses the reference's own 2D DFD output by one ulp.)
+template <int D>
+__device__ __forceinline__ double sq_sum(const double* t) {
+  static_assert(D >= 2, "two or more coordinates");
+  double s = __fma_rn(t[0], t[0], __dmul_rn(t[1], t[1]));
+#pragma unroll
+  for (int k = 2; k < D; ++k) s = __fma_rn(t[k], t[k], s);
+  return s;
+}
 
 template <int D>
 __device__ __forceinline__ double dist_sq(const double* a, const double* b) {
-  double s = 0.0;
+  double t[D];
 #pragma unroll
-  for (int k = 0; k < D; ++k) {
-    const double t = __dsub_rn(a[k], b[k]);
-    s = __fma_rn(t, t, s);
-  }
-  return s;
+  for (int k = 0; k < D; ++k) t[k] = __dsub_rn(a[k], b[k]);
+  return sq_sum<D>(t);
 }
 
 // Squared distance from x to the segment a -> a + ab with ab2 = |ab|^2 (VE-FD weights,
@@ -193,13 +205,10 @@ __device__ __forceinline__ double pt_seg_sq(const double* x, const double* a, co
   for (int k = 0; k < D; ++k) apab = __fma_rn(__dsub_rn(x[k], a[k]), ab[k], apab);
   double t = __ddiv_rn(apab, ab2);
   t = fmin(1.0, fmax(0.0, t));
-  double w = 0.0;
+  double dd[D];
 #pragma unroll
-  for (int k = 0; k < D; ++k) {
-    const double dd = __dsub_rn(x[k], __fma_rn(t, ab[k], a[k]));
-    w = __fma_rn(dd, dd, w);
-  }
-  return w;
+  for (int k = 0; k < D; ++k) dd[k] = __dsub_rn(x[k], __fma_rn(t, ab[k], a[k]));
+  return sq_sum<D>(dd);
 }
 
 // Free interval on segment a -> a + di inside the ball of radius^2 r2 around x
@@ -210,14 +219,14 @@ template <int D>
 __device__ __forceinline__ void free_interval(const double* x, const double* a, const double* di,
                                               double A, double inv2A, double r2, double& lo,
                                               double& hi, bool mat = false) {
-  double B = 0.0, Cc = mat ? 0.0 : -r2;
+  double B = 0.0, Cc = -r2, m[D];
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    const double mi = __dsub_rn(a[k], x[k]);
-    B = __fma_rn(mi, di[k], B);
-    Cc = __fma_rn(mi, mi, Cc);
+    m[k] = __dsub_rn(a[k], x[k]);
+    B = __fma_rn(m[k], di[k], B);
+    Cc = __fma_rn(m[k], m[k], Cc);
   }
-  if (mat) Cc = __dsub_rn(Cc, r2);
+  if (mat) Cc = __dsub_rn(sq_sum<D>(m), r2);
   B = __dmul_rn(B, 2.0);
   const double disc = __fma_rn(B, B, -__dmul_rn(__dmul_rn(4.0, A), Cc));
   lo = -1.0;

@@ -634,22 +634,20 @@ __global__ void prep_kernel(const PairDesc* pairs, PairState* st, int npairs, in
     double2* rowc = const_cast<double2*>(pd.rowc);
     double2* colrec = const_cast<double2*>(pd.colrec);
     for (int i = threadIdx.x; i < pd.n1 - 1; i += blockDim.x) {
-      double A = 0.0;
-      for (int k = 0; k < d; ++k) {
-        const double t = __dsub_rn(pd.P[(size_t)(i + 1) * d + k], pd.P[(size_t)i * d + k]);
-        A = __fma_rn(t, t, A);
-      }
+      double t[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < d; ++k)
+        t[k] = __dsub_rn(pd.P[(size_t)(i + 1) * d + k], pd.P[(size_t)i * d + k]);
+      const double A = d == 3 ? sq_sum<3>(t) : sq_sum<2>(t);
       rowc[i] = make_double2(A, __ddiv_rn(0.5, A));
     }
     for (int j = threadIdx.x; j < pd.n2 - 1; j += blockDim.x) {
-      double A = 0.0;
-      double q0[3] = {0, 0, 0}, q1[3] = {0, 0, 0};
+      double q0[3] = {0, 0, 0}, q1[3] = {0, 0, 0}, t[3] = {0, 0, 0};
       for (int k = 0; k < d; ++k) {
         q0[k] = pd.Q[(size_t)j * d + k];
         q1[k] = pd.Q[(size_t)(j + 1) * d + k];
-        const double t = __dsub_rn(q0[k], q1[k]);  // reference stages q_j - q_{j+1} (.cu:1137)
-        A = __fma_rn(t, t, A);
+        t[k] = __dsub_rn(q0[k], q1[k]);  // reference stages q_j - q_{j+1} (.cu:1137)
       }
+      const double A = d == 3 ? sq_sum<3>(t) : sq_sum<2>(t);
       const double inv = __ddiv_rn(0.5, A);
       if (d == 2) {
         double2* r = colrec + (size_t)j * 3;
