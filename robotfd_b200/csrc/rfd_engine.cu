@@ -755,6 +755,9 @@ void launch_team(const rfd_context* ctx, const WaveArgs& wa, cudaStream_t st) {
     team_kernel<KIND, 8><<<ctx->team_grid[KIND], 256, team_smem_bytes<KIND>(), st>>>(wa);
 }
 
+// Row of rfd_context::team_grids for a team shape.
+int team_shape_index(int warps) { return warps == 4 ? 0 : 1; }
+
 int ring_of(int64_t strips, int rows) {  // strips - 1 rows are handed over; at least 1
   return (int)std::max<int64_t>(1, std::min<int64_t>(strips - 1, rows));
 }
@@ -1553,10 +1556,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                         cudaMemcpyDeviceToHost));
     fprintf(stderr,
             "rfd prof (Mcycles): in_wait %.1f jump %.1f tile_wait %.1f steps %.1f strip_total %.1f |"
-            " chunks %llu jumps %llu strips %llu | helpers: tile %.1f req_wait %.1f tiles %llu |"
-            " flush %.1f flushes %llu\n",
+            " chunks %llu jumps %llu strips %llu | helpers: tile %.1f (staging %.1f) req_wait %.1f"
+            " tiles %llu | flush %.1f flushes %llu\n",
             pc[0] / 1e6, pc[1] / 1e6, pc[2] / 1e6, pc[3] / 1e6, pc[4] / 1e6, pc[5], pc[6], pc[7],
-            pc[8] / 1e6, pc[9] / 1e6, pc[10], pc[11] / 1e6, pc[12]);
+            pc[8] / 1e6, pc[13] / 1e6, pc[9] / 1e6, pc[10], pc[11] / 1e6, pc[12]);
     // strip chain of the first pair: handoff = first live input of strip s after the first
     // live output of strip s-1; lag = first live output of strip s after its first live input
     // (lag split: input -> its tile taken -> its steps done -> the next chunk's input in hand
@@ -1711,13 +1714,19 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], team_kernel<K_DEC, 4>, 128, sm_dec);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], team_kernel<K_VEFD, 8>, 256, sm_ve);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], team_kernel<K_DEC, 8>, 256, sm_dec);
+    // RFD_TEAM_PER_SM (1 or more): caps the teams resident per SM (the grid is persistent)
+    if (const char* tp = getenv("RFD_TEAM_PER_SM")) {
+      const int cap = atoi(tp);
+      if (cap >= 1)
+        for (int k = 0; k < 4; ++k) o[k] = std::min(std::max(1, o[k]), cap);
+    }
     c->team_grids[0][K_VEFD] = std::max(1, o[0]) * c->num_sms;
     c->team_grids[0][K_DEC] = std::max(1, o[1]) * c->num_sms;
     c->team_grids[1][K_VEFD] = std::max(1, o[2]) * c->num_sms;
     c->team_grids[1][K_DEC] = std::max(1, o[3]) * c->num_sms;
     const char* tw = getenv("RFD_TEAM_WARPS");
-    c->team_warps = tw && tw[0] == '4' && !tw[1] ? 4 : 8;
-    for (int k = 0; k < 3; ++k) c->team_grid[k] = c->team_grids[c->team_warps == 4 ? 0 : 1][k];
+    c->team_warps = tw && strcmp(tw, "4") == 0 ? 4 : 8;
+    for (int k = 0; k < 3; ++k) c->team_grid[k] = c->team_grids[team_shape_index(c->team_warps)][k];
     const char* e = getenv("RFD_SOLO");
     c->solo = e && e[0] == '1';
     const char* ls = getenv("RFD_LOCKSTEP");
@@ -2008,7 +2017,7 @@ int32_t rfd_autotune_search(rfd_context* ctx, int64_t npairs, const double* cons
         }
       }
   ctx->team_warps = rc == RFD_OK ? bw : keep_w;
-  for (int k = 0; k < 3; ++k) ctx->team_grid[k] = ctx->team_grids[ctx->team_warps == 4 ? 0 : 1][k];
+  for (int k = 0; k < 3; ++k) ctx->team_grid[k] = ctx->team_grids[team_shape_index(ctx->team_warps)][k];
   ctx->search_switch = rc == RFD_OK ? bs : keep_sw;
   ctx->search_window = rc == RFD_OK ? bn : keep_win;
   ctx->timing = keep_timing;

@@ -180,6 +180,7 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     if (lane == 0) mbar_arrive(&sh->staged);
     if (!mbar_wait(&sh->staged, seqS & 1, wa, t0)) break;
     ++seqS;
+    if (wa.prof && lane == 0) atomicAdd(&wa.prof[13], (unsigned long long)(clock64() - tc0));
     // column j = c*32 + u - lane sits at jj = u - lane + 31 of the staged rows
     auto col_at = [&](int u, ColRec<KIND, D>& col) {
       const int jj = u - lane + 31;
