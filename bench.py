@@ -44,7 +44,7 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
 DEC_DRAM_BYTES_20K = 3.730432e6   # ncu, one decision launch of the 20,000-point case
 VEFD_DRAM_BYTES_20K = 4.31e6      # ncu, one VE-FD launch of the same case (two launches averaged)
 COARSE_UB = 6  # the learned form's upper bound: inflated DFD of every 6th point (rfd.h coarse_ub)
-DFD_DRAM_BYTES_200K = 1.10e9 + 1.20e9
+DFD_DRAM_BYTES_200K = 31.5e6 + 68.4e6  # ncu, the exact DFD launch of the long pair (32-row ring)
 KERNEL_OF_PHASE = {"dfd": f"dfd_kernel<{'1, INFL' if COARSE_UB else '8'}>",
                    "vefd": "team_kernel<K_VEFD>", "search": "team_kernel<K_DEC>"}
 FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3 + (4 if COARSE_UB else 0),  # + sqrt, 2 adds, square
@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--profile-search", type=int, default=0, metavar="N",
                     help="profiling case: one batched call of the learned form (every probe) on "
                          "the first N pairs of the uneven batch, then exit (no JSON line)")
+    ap.add_argument("--profile-bounds", type=int, default=0, metavar="N",
+                    help="profiling case: N calls of the exact bounds (DFD, then VE-FD pruned by "
+                         "it) on the long pair of --points points, then exit (no JSON line)")
     return ap.parse_args()
 
 
@@ -450,6 +453,13 @@ def main():
         ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True, max_probes=1)
         ctx.close()
         return
+    if args.profile_bounds:
+        P, Q = workload(args.points)
+        ctx = rfd.Context(0)
+        for _ in range(args.profile_bounds):
+            ctx.bounds(P, Q, quirks=False)
+        ctx.close()
+        return
     if args.profile_search:
         pairs = batch_pairs()[: args.profile_search]
         ctx = rfd.Context(0)
@@ -565,9 +575,8 @@ def main():
         traffic = per20k * (n1 + n2) / 40000
     elif dom == "dfd" and not COARSE_UB:
         # ncu dram__bytes_read.sum + dram__bytes_write.sum of the DFD launch on the full
-        # 200,000-point pair (one pass): the boundary rows the 256-row strips hand over,
-        # scaled by their count for other sizes
-        traffic = DFD_DRAM_BYTES_200K * ((n1 + 255) // 256 - 1) * n2 / (781 * 200000)
+        # 200,000-point pair (one pass): curves and the ring rows L2 evicts, scaled by points
+        traffic = DFD_DRAM_BYTES_200K * (n1 + n2) / 400000
     sm_mhz = clk.get("sm_mhz") or 1965.0
     pcalls = max(pphase["calls"], 1)
 
