@@ -44,6 +44,7 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
 DEC_DRAM_BYTES_20K = 3.730432e6   # ncu, one decision launch of the 20,000-point case
 VEFD_DRAM_BYTES_20K = 4.31e6      # ncu, one VE-FD launch of the same case (two launches averaged)
 COARSE_UB = 6  # the learned form's upper bound: inflated DFD of every 6th point (rfd.h coarse_ub)
+ARITY = 4  # batched forms: radii per round for the longest-chain pairs (rfd.h search_arity)
 DFD_DRAM_BYTES_200K = 31.5e6 + 68.4e6  # ncu, the exact DFD launch of the long pair (32-row ring)
 KERNEL_OF_PHASE = {"dfd": f"dfd_kernel<{'1, INFL' if COARSE_UB else '8'}>",
                    "vefd": "team_kernel<K_VEFD>", "search": "team_kernel<K_DEC>"}
@@ -295,21 +296,26 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
     ctx.distance_batch(Ps[:64], Qs[:64], precise=True, model=model)  # warm
     # the batched forms run as CUDA graphs: the first (untimed) call captures, the timed
     # calls with the same layout replay
-    batched = dict(precise=True, model=model, graph=True)
+    batched = dict(precise=True, model=model, graph=True, search_arity=ARITY)
     ctx.distance_batch(Ps, Qs, **batched)
     t_l, learned = timed(lambda: ctx.distance_batch(Ps, Qs, **batched), 2)
+    # the same with plain bisection rounds (one radius per probe)
+    bisect = dict(batched, search_arity=0)
+    ctx.distance_batch(Ps, Qs, **bisect)
+    t_b, learned_b = timed(lambda: ctx.distance_batch(Ps, Qs, **bisect), 2)
     # the north star's target form: batched, learned bracket, mixed precision (FP32 filter)
     mixed = dict(batched, precision=rfd.RFD_PREC_FP32_FILTER)
     ctx.distance_batch(Ps, Qs, **mixed)
     t_m, learned_mixed = timed(lambda: ctx.distance_batch(Ps, Qs, **mixed), 2)
     # untimed first call: the coarse pairs' arrays can grow the context's workspace once
-    ctx.distance_batch(Ps, Qs, precise=True, model=model, coarse_ub=COARSE_UB)
+    ctx.distance_batch(Ps, Qs, precise=True, model=model, coarse_ub=COARSE_UB,
+                       search_arity=ARITY)
     t_c, _ = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
-                                              coarse_ub=COARSE_UB), 1)
+                                              coarse_ub=COARSE_UB, search_arity=ARITY), 1)
     t_p, plain = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True), 1)
     # the same search without the network: the threshold probe over VE-FD alone (a bracket at
     # the VE-FD bound), as a replayed graph like the learned form
-    alone = dict(precise=True, graph=True,
+    alone = dict(precise=True, graph=True, search_arity=ARITY,
                  brackets=[(r["vefd"] * (1 - 1e-15), r["vefd"]) for r in plain])
     ctx.distance_batch(Ps, Qs, **alone)
     t_a, thr = timed(lambda: ctx.distance_batch(Ps, Qs, **alone), 2)
@@ -327,6 +333,7 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
     for k, r in zip(idx, single):
         assert r["distance"] == plain[k]["distance"], "single and batched plain results differ"
     sps = {"learned_batched": n / (statistics.median(t_l) * 1e-3),
+           "learned_batched_bisection": n / (statistics.median(t_b) * 1e-3),
            "learned_batched_mixed": n / (statistics.median(t_m) * 1e-3),
            "learned_batched_coarse_ub": n / (t_c[0] * 1e-3),
            "plain_batched": n / (statistics.median(t_p) * 1e-3),
@@ -351,8 +358,12 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
                      "search_ms": {f"w{w}_s{['quarter', 'teams', 'queue'][si]}_win{win}":
                                    round(v, 2) for (w, si, win), v in tuned_search["ms"].items()}},
         "cuda_graph": "batched forms captured once and replayed (rfd_options.graph)",
+        "search_arity": f"{ARITY} radii per round for the 32 longest-chain pairs once few pairs "
+                        "remain (rfd_options.search_arity), in every learned and threshold-only "
+                        "form; plain_batched and learned_batched_bisection bisect",
         "plain_single_sample": f"{len(idx)} pairs (every {n // len(idx)}th), one call each",
         "mean_probes": {"learned": statistics.mean(r["probes"] for r in learned),
+                        "learned_bisection": statistics.mean(r["probes"] for r in learned_b),
                         "plain": statistics.mean(r["probes"] for r in plain),
                         "threshold_only": statistics.mean(r["probes"] for r in thr)},
         "tail_pairs": {"count": len(tail),

@@ -19,6 +19,8 @@ extern "C" {
 #endif
 
 #define RFD_ABI_VERSION 1
+#define RFD_MAX_ARITY 8    /* rfd_options.search_arity */
+#define RFD_ARITY_PAIRS 32 /* pairs per call that get k-ary rounds */
 #define RFD_MAX_PROBES 200
 
 /* Status codes (the reference prints CUDA errors and carries on; this ABI reports them). */
@@ -115,6 +117,17 @@ typedef struct rfd_options {
                                it instead of issuing each launch.  Results are identical. */
   int32_t formula;          /* enum rfd_formula, default RFD_FORMULA_FUSED.  The FP32 filter
                                certifies the fused intervals only: it needs RFD_FORMULA_FUSED. */
+  int32_t search_arity;     /* 0 or 1 (default): every probe is one decision at the bisection's
+                               midpoint (the reference's search, src/frechet.cpp:36-63).  K in
+                               [2, RFD_MAX_ARITY] (batches, rfd_distance_batch): the pairs whose
+                               probe chains are longest (up to RFD_ARITY_PAIRS per call) get K - 1
+                               extra decision workspaces, and once few pairs remain (at most the
+                               teams / (2K), or RFD_ARITY_GATE) each of their bisection rounds
+                               decides K radii at once, splitting the bracket into K + 1 parts
+                               (about log2(K + 1) halvings per round instead of one).  Only the
+                               probe sequence changes: every decision is the same function of its
+                               radius, the stop rule is the same, and result.probes counts every
+                               decision. */
 } rfd_options;
 
 typedef struct rfd_result {

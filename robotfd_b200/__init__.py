@@ -86,6 +86,7 @@ class Options(ctypes.Structure):
         ("drop_repeats", ctypes.c_int32),
         ("graph", ctypes.c_int32),
         ("formula", ctypes.c_int32),
+        ("search_arity", ctypes.c_int32),
     ]
 
 
@@ -235,7 +236,7 @@ def _curve(c):
 
 def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, memory=RFD_MEM_HOST,
             precision=RFD_PREC_FP64, model=None, coarse_ub=0, drop_repeats=False, graph=False,
-            formula=0):
+            formula=0, search_arity=0):
     o = Options()
     lib().rfd_options_init(ctypes.byref(o), 1 if precise else 0)
     o.dense = int(bool(dense))
@@ -252,6 +253,7 @@ def options(precise=False, dense=False, max_probes=64, tol=None, quirks=None, me
     o.drop_repeats = int(bool(drop_repeats))
     o.graph = int(bool(graph))
     o.formula = int(formula)
+    o.search_arity = int(search_arity)
     return o
 
 

@@ -41,7 +41,8 @@ enum Phase : int {
   PH_VEFD_DENSE = 2,
   PH_SEARCH = 3,
   PH_DONE = 4,
-  PH_BRACKET = 5  // waiting for the learned bracket
+  PH_BRACKET = 5,  // waiting for the learned bracket
+  PH_KWAIT = 6     // k-ary round: this decision is done, the round's others are not
 };
 
 // Progress record of a strip's output boundary.
@@ -100,6 +101,15 @@ struct PairState {
   int formula;  // decision intervals: 0 the fused path's, 1 the materialised path's (rfd.h)
   int pushed;      // continuous search: queue entries of the running probe so far (<= strips)
   int next_strip;  // continuous search: strips of the running probe taken so far
+  unsigned long long t_done;  // %globaltimer (ns) when the pair's search ended (RFD_PROF report)
+  // k-ary rounds of the continuous search (rfd_options.search_arity).  A pair with members
+  // owns kary_cap extra decision workspaces, whose states are st[kary_base ..]; every state of
+  // such a group (the pair's own included) has kary_real = the pair's index.
+  int kary_real, kary_base, kary_cap;
+  int kary_n;     // the pair: decisions of the running round (0: plain probe)
+  int kary_left;  // the pair: decisions of the round still running
+  int kary_in;    // this decision belongs to a round
+  int kary_reach; // its outcome
 };
 
 template <int D>
@@ -130,6 +140,8 @@ struct WaveArgs {
   int gate_min;
   int window;        // continuous search: strips a probe queues at its start, at least,
   int window_teams;  // ... and at least this over the active pairs (a lone pair: its teams)
+  int kary_k;        // continuous search: radii per k-ary round (< 2: none)
+  int kary_gate;     // ... run while at most this many pairs are active
 };
 
 // ------------------------------------------------------------------ memory helpers

@@ -69,6 +69,7 @@ __device__ __forceinline__ void begin_search(PairState* st, int* active_pairs,
 __device__ __forceinline__ void next_probe(PairState* st, int* active_pairs);
 
 __device__ __forceinline__ void finish_pair(PairState* st, int* active_pairs) {
+  st->t_done = global_ns();
   st->phase = PH_DONE;
   st->active = 0;
   st->distance = (st->srch.ub + st->srch.lb) / 2.0;
@@ -145,6 +146,11 @@ __device__ void finalize(PairState* st, const PairDesc& pd, int* active_pairs) {
       st->phase = PH_DONE;
       st->active = 0;
       atomicSub(active_pairs, 1);
+    } else if (st->kary_in) {
+      // one decision of a k-ary round: its outcome waits for the round's others (kary_done)
+      st->kary_reach = r == 1.0;
+      st->kary_in = 0;
+      st->phase = PH_KWAIT;
     } else {
       search_update(st->srch, st->split, r == 1.0);  // reference .cu:1592, frechet.cpp:80-85
       next_probe(st, active_pairs);
@@ -383,6 +389,21 @@ __global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int 
   }
 }
 
+// The k-ary members' boundary rows (descriptors first .. first + count - 1) to the
+// "not yet written" pattern, before the continuous search.
+__global__ void member_fill_kernel(const PairDesc* pairs, int first, int count) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int v = blockIdx.y; v < count; v += gridDim.y) {
+    const PairDesc pd = pairs[first + v];
+    const long long S = (pd.n1 - 1 + 31) / 32;
+    if (S < 2) continue;
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(pd.bnd);
+    const long long n = (S - 1) * pd.cstride;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+      b[k] = kBndEmpty;
+  }
+}
+
 // Dense DFD strips of 32*K rows (rfd_dfd.cuh), same in-order ticket scheme as wave_kernel
 // over the (pair, 32-row strip) item list: item (p, s) is strip s of 32*K rows, items past
 // the pair's last tall strip are skipped.
@@ -451,6 +472,97 @@ __device__ void start_probe(const WaveArgs& wa, PairState* st, int p, int S) {
   __threadfence();
   queue_strips(wa, st, p, S,
                max(wa.window, wa.window_teams / max(1, ld_volatile(wa.active_pairs))));
+}
+
+// ---- k-ary rounds of the continuous search (rfd_options.search_arity)
+//
+// A pair with members (extra decision workspaces, st[kary_base ..]) decides, once few pairs
+// remain and its search is plain bisection, n radii per round that split (lb, ub) into n + 1
+// equal parts; the round's last decision to end combines the outcomes (kary_done): the
+// smallest reachable radius is the new ub, the largest unreachable one below it the new lb.
+// Every decision is the same function of its radius as a bisection probe's.
+constexpr int kMaxArity = RFD_MAX_ARITY;
+
+__device__ PairState* kary_member(const WaveArgs& wa, PairState* g, int m) {
+  return m == 0 ? g : wa.st + g->kary_base + (m - 1);
+}
+
+// Starts pair p's next probe (phase PH_SEARCH, split set by next_probe): one decision, or a
+// k-ary round.  One thread.
+__device__ void start_next(const WaveArgs& wa, PairState* g, int p, int S) {
+  int n = 1;
+  if (g->kary_cap > 0 && wa.kary_k >= 2 && g->srch.mode == SM_BISECT &&
+      ld_volatile(wa.active_pairs) <= wa.kary_gate) {
+    // the widest round whose decisions still close the gap within the probe cap: halvings
+    // left h, rounds of n radii take ceil(h / log2(n + 1)) of them
+    const Search& q = g->srch;
+    const double w = q.stop_mode == 0 ? q.tol : q.tol * q.ub;
+    const double h = w > 0.0 ? ceil(log2(fmax((q.ub - q.lb) / w, 1.0))) : 64.0;
+    const int budget = q.max_probes - q.probes;
+    for (n = min(wa.kary_k, g->kary_cap + 1); n >= 2; --n)
+      if (ceil(h / log2((double)(n + 1))) * n <= (double)budget) break;
+    n = max(n, 1);
+  }
+  double r[kMaxArity];
+  int m = 0;
+  if (n >= 2) {
+    // n radii strictly inside (lb, ub) and increasing (fewer where doubles run out)
+    double prev = g->srch.lb;
+    for (int i = 1; i <= n; ++i) {
+      const double x = g->srch.lb + (g->srch.ub - g->srch.lb) * ((double)i / (double)(n + 1));
+      if (x > prev && x < g->srch.ub) r[m++] = prev = x;
+    }
+  }
+  if (m < 2) {
+    start_probe(wa, g, p, S);
+    return;
+  }
+  g->kary_n = m;
+  g->kary_left = m;
+  for (int k = 0; k < m; ++k) {
+    PairState* ms = kary_member(wa, g, k);
+    ms->split = r[k];
+    ms->r2 = __dmul_rn(r[k], r[k]);
+    ms->kary_in = 1;
+    ms->phase = PH_SEARCH;
+    ms->active = 1;
+  }
+  __threadfence();
+  for (int k = 0; k < m; ++k)
+    start_probe(wa, kary_member(wa, g, k), k == 0 ? p : g->kary_base + (k - 1), S);
+}
+
+// A decision of a k-ary round ended (its boundary words are cleared); the round's last one
+// combines the outcomes and starts the pair's next probe.  One thread.
+__device__ void kary_done(const WaveArgs& wa, PairState* ms, int S) {
+  const int p = ms->kary_real;
+  PairState* g = wa.st + p;
+  __threadfence();
+  if (atomicSub(&g->kary_left, 1) != 1) return;
+  __threadfence();
+  const int n = g->kary_n;
+  double ub = g->srch.ub, lb = g->srch.lb;
+  for (int k = 0; k < n; ++k) {
+    const PairState* m = kary_member(wa, g, k);
+    if (ld_volatile(&m->kary_reach) && m->split < ub) ub = m->split;
+  }
+  for (int k = 0; k < n; ++k) {
+    const PairState* m = kary_member(wa, g, k);
+    if (!ld_volatile(&m->kary_reach) && m->split < ub && m->split > lb) lb = m->split;
+  }
+  for (int k = 1; k < n; ++k) {
+    PairState* m = kary_member(wa, g, k);
+    g->cells_eval += m->cells_eval;
+    g->cells_fp64 += m->cells_fp64;
+    g->cells_nominal += m->cells_nominal;
+    m->cells_eval = m->cells_fp64 = m->cells_nominal = 0;
+  }
+  g->srch.lb = lb;
+  g->srch.ub = ub;
+  g->srch.probes += n;
+  g->kary_n = 0;
+  next_probe(g, wa.active_pairs);
+  if (g->phase == PH_SEARCH && g->active) start_next(wa, g, p, S);
 }
 
 // Continuous search: the first strips of every pair in the search phase.
@@ -559,6 +671,7 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
           finalize<KIND>(st, pd, wa.active_pairs);
           __threadfence();
           if (dyn && st->phase == PH_SEARCH && st->active) sh->push = 1;
+          else if (dyn && st->phase == PH_KWAIT) sh->push = 2;
         }
       }
     }
@@ -575,7 +688,10 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
       }
       __threadfence();
       __syncthreads();
-      if (threadIdx.x == 0) start_probe(wa, st, p, S);
+      if (threadIdx.x == 0) {
+        if (sh->push == 1) start_next(wa, st, p, S);
+        else kary_done(wa, st, S);
+      }
     }
   }
 }
@@ -1005,8 +1121,6 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     trv[p] = n1s[p] >= 2 && n2s[p] >= 2 && n1s[p] > n2s[p];
   auto trows = [&](int64_t p) { return trv[p] ? n2s[p] : n1s[p]; };
   auto tcols = [&](int64_t p) { return trv[p] ? n1s[p] : n2s[p]; };
-  L.tdescs = take(sizeof(PairDesc) * npairs);
-  L.states = take(sizeof(PairState) * npairs);
   // items: interleave pairs by strip index so early strips of every pair go first
   std::vector<int> order(npairs);
   for (int64_t p = 0; p < npairs; ++p) order[p] = (int)p;
@@ -1036,6 +1150,36 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     if (dyn_cap * (int64_t)sizeof(unsigned long long) > ((int64_t)512 << 20)) dyn_cap = 0;
   }
   const size_t dyn_off = dyn_cap ? take(sizeof(unsigned long long) * dyn_cap) : 0;
+  // k-ary rounds (rfd_options.search_arity = K): the pairs whose probe chains are longest get
+  // K - 1 member decisions each (descriptor, state and boundary rows of their own, after the
+  // pairs' in the same arrays).  A decision's chain is about max(strips x 7 us, 32-column
+  // chunks x 3 us) on a B200; members of more than 256 MB are not given.
+  const int karity = (dyn_cap && mode == MODE_DISTANCE && o.search_arity >= 2)
+                         ? std::min<int>(o.search_arity, RFD_MAX_ARITY) : 0;
+  std::vector<int64_t> kpairs;
+  if (karity) {
+    std::vector<std::pair<double, int64_t>> est;
+    for (int64_t p = 0; p < npairs; ++p) {
+      if (n1s[p] < 2 || n2s[p] < 2) continue;
+      const int64_t St = (trows(p) - 1 + 31) / 32, C = tcols(p);
+      const double bytes = 8.0 * (double)std::max<int64_t>(St - 1, 1) * (double)align_up((size_t)C, 32) +
+                           4.0 * (double)std::max<int64_t>(St - 1, 1) * (double)(C / 32 + 64) +
+                           (double)sizeof(Prog) * (double)St;
+      if (bytes > 256.0 * (1 << 20)) continue;
+      est.push_back({std::max(7.0 * (double)St, 3.0 * (double)((C + 31) / 32)), p});
+    }
+    std::stable_sort(est.begin(), est.end(), [](const std::pair<double, int64_t>& a,
+                                                const std::pair<double, int64_t>& b) {
+      return a.first > b.first;
+    });
+    for (size_t k = 0; k < est.size() && k < (size_t)RFD_ARITY_PAIRS; ++k)
+      kpairs.push_back(est[k].second);
+  }
+  const int64_t nmem = (int64_t)kpairs.size() * (karity > 1 ? karity - 1 : 0);
+  const int64_t nst = npairs + nmem;  // descriptors and states: the pairs', then the members'
+  auto mpair = [&](int64_t v) { return kpairs[v / (karity - 1)]; };
+  L.tdescs = take(sizeof(PairDesc) * nst);
+  L.states = take(sizeof(PairState) * nst);
   // ticket counters: DFD, two VE-FD, probe rounds (+1 for a decision), the continuous
   // search's ticket and queue tail; then a gate word per probe round
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
@@ -1057,6 +1201,14 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     L.tags[p] = take(sizeof(unsigned) * L.ring_t[p] * tstride);
     L.prog[p] = take(sizeof(Prog) * std::max<int64_t>(St, (trows(p) + 31) / 32));
     L.slots[p] = take(sizeof(unsigned long long) * (n1s[p] + 31) / 32);  // a count per DFD strip
+  }
+  std::vector<size_t> mtags(nmem), mprog(nmem), mbnd(nmem);
+  for (int64_t v = 0; v < nmem; ++v) {
+    const int64_t p = mpair(v);
+    const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
+    const int64_t tstride = align_up((size_t)((tcols(p) + 31) / 32), 32);
+    mtags[v] = take(sizeof(unsigned) * ring_of(St, INT32_MAX) * tstride);
+    mprog[v] = take(sizeof(Prog) * std::max<int64_t>(St, 1));
   }
   L.zero_end = off;
   L.active = take(sizeof(int));
@@ -1094,14 +1246,19 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       cQ[p] = take(sizeof(double) * (full ? n2 : coarse_n(n2)) * (d + 1));
     }
   }
+  for (int64_t v = 0; v < nmem; ++v) {
+    const int64_t p = mpair(v);
+    const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
+    mbnd[v] = take(sizeof(double) * ring_of(St, INT32_MAX) * align_up((size_t)tcols(p), 32));
+  }
   L.total = off;
 
   size_t hoff = 0;
   auto htake = [&](size_t bytes) { size_t r = hoff; hoff = align_up(hoff + bytes, 256); return r; };
   L.h_descs = htake(sizeof(PairDesc) * npairs);
   const size_t h_cdescs = ck ? htake(sizeof(PairDesc) * npairs) : 0;
-  L.h_tdescs = htake(sizeof(PairDesc) * npairs);
-  L.h_states = htake(sizeof(PairState) * npairs);
+  L.h_tdescs = htake(sizeof(PairDesc) * nst);
+  L.h_states = htake(sizeof(PairState) * nst);
   L.h_items = htake(sizeof(int2) * nitems);
   L.h_titems = htake(sizeof(int2) * ntitems);
   L.h_misc = htake(4 * sizeof(int));
@@ -1115,12 +1272,18 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   }
   L.h_total = hoff;
 
-  int rc = ensure_device(ctx, L.total);
+  // RFD_GUARD=1 (debugging): a guard band after the workspace, filled with a pattern before the
+  // call's launches and checked after them; a changed byte means a write past the workspace
+  const size_t guard = getenv("RFD_GUARD") ? ((size_t)8 << 20) : 0;
+  int rc = ensure_device(ctx, L.total + guard);
   if (rc) return rc;
   rc = ensure_host(ctx, L.h_total);
   if (rc) return rc;
   char* dbase = (char*)ctx->dws;
   char* hbase = (char*)ctx->hws;
+  if (guard) {
+    RFD_CUDA(cudaMemsetAsync(dbase + L.total, 0xA5, guard, ctx->stream));
+  }
 
   // ---------------- host staging
   PairDesc* hd = (PairDesc*)(hbase + L.h_descs);
@@ -1204,6 +1367,33 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       s.r2 = radius * radius;
     }
   }
+  // k-ary members: the pair's team descriptor with boundary rows, tags and progress words of
+  // their own; states idle (PH_KWAIT) until a round starts them
+  for (int64_t v = 0; v < nmem; ++v) {
+    const int64_t p = mpair(v), idx = npairs + v;
+    PairDesc* td = (PairDesc*)(hbase + L.h_tdescs);
+    td[idx] = td[p];
+    td[idx].bnd = (double*)(dbase + mbnd[v]);
+    td[idx].tags = (unsigned*)(dbase + mtags[v]);
+    td[idx].prog = (Prog*)(dbase + mprog[v]);
+    PairState& m = hs[idx];
+    memset(&m, 0, sizeof(m));
+    m.quirks = hs[p].quirks;
+    m.dense = hs[p].dense;
+    m.filter = hs[p].filter;
+    m.formula = hs[p].formula;
+    m.use_model = hs[p].use_model;
+    m.epoch = 1;
+    m.dead_from = INT_MAX;
+    m.U = (double)INFINITY;
+    m.phase = PH_KWAIT;
+    m.kary_real = (int)p;
+    if (v % (karity - 1) == 0) {
+      hs[p].kary_real = (int)p;
+      hs[p].kary_base = (int)idx;
+      hs[p].kary_cap = karity - 1;
+    }
+  }
   {
     int64_t k = 0;
     for (int64_t sidx = 0; sidx < maxS; ++sidx)
@@ -1263,10 +1453,14 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
 
   // ---------------- transfers
   cudaStream_t st = ctx->stream;
-  size_t h2d_bytes = 2 * sizeof(PairDesc) * npairs + sizeof(PairState) * npairs +
+  size_t h2d_bytes = sizeof(PairDesc) * (npairs + nst) + sizeof(PairState) * nst +
                      sizeof(int2) * (nitems + ntitems) + sizeof(int);
   if (!on_device)
     for (int64_t p = 0; p < npairs; ++p) h2d_bytes += sizeof(double) * (n1s[p] + n2s[p]) * dims[p];
+  // k-ary rounds run while at most kary_gate pairs are active (RFD_ARITY_GATE, read per call)
+  int kary_gate = std::max(1, ctx->team_grid[K_DEC] / std::max(1, 2 * karity));
+  if (const char* kg = getenv("RFD_ARITY_GATE"))
+    if (atoi(kg) >= 1) kary_gate = atoi(kg);
   int* hmisc = (int*)(hbase + L.h_misc);  // [0] active pairs, [1] error word read back
   hmisc[0] = (int)npairs;
   hmisc[1] = 0;
@@ -1294,11 +1488,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                                cudaMemcpyHostToDevice, st));
       h2d_bytes += sizeof(PairDesc) * npairs;
     }
-    RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * npairs,
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.states, hbase + L.h_states, sizeof(PairState) * nst,
                              cudaMemcpyHostToDevice, st));
     RFD_CUDA(cudaMemcpyAsync(dbase + L.items, hbase + L.h_items, sizeof(int2) * nitems,
                              cudaMemcpyHostToDevice, st));
-    RFD_CUDA(cudaMemcpyAsync(dbase + L.tdescs, hbase + L.h_tdescs, sizeof(PairDesc) * npairs,
+    RFD_CUDA(cudaMemcpyAsync(dbase + L.tdescs, hbase + L.h_tdescs, sizeof(PairDesc) * nst,
                              cudaMemcpyHostToDevice, st));
     RFD_CUDA(cudaMemcpyAsync(dbase + L.titems, hbase + L.h_titems, sizeof(int2) * ntitems,
                              cudaMemcpyHostToDevice, st));
@@ -1457,9 +1651,17 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       wa.dyn_cap = dyn_cap;
       wa.window = ctx->search_window;
       wa.window_teams = ctx->team_grid[K_DEC];
+      wa.kary_k = karity;
+      wa.kary_gate = kary_gate;
       const int nstatic = wa.nitems;
       wa.nitems = 0;  // every strip comes from the queue
       fill(PH_SEARCH);
+      if (nmem) {  // the members' boundary rows: not yet written
+        member_fill_kernel<<<dim3(64, (unsigned)std::min<int64_t>(nmem, 1024)), 256, 0, st>>>(
+            dt, (int)npairs, (int)nmem);
+        RFD_CUDA(cudaGetLastError());
+        ++launches;
+      }
       search_queue_init_kernel<<<(int)std::min<int64_t>((npairs + 255) / 256, 1024), 256, 0, st>>>(
           dt, ds, (int)npairs, wa);
       launch_team<K_DEC>(ctx, wa, st);
@@ -1501,7 +1703,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
                          ctx->search_switch, ctx->search_window, ctx->team_warps,
                          (int)(ctx->spin_cycles >> 32),
-                         (int)(ctx->spin_cycles & 0xffffffff)};
+                         (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));
@@ -1546,6 +1748,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   RFD_CUDA(cudaStreamSynchronize(st));
+  if (guard) {
+    std::vector<unsigned char> g(guard);
+    RFD_CUDA(cudaMemcpy(g.data(), dbase + L.total, guard, cudaMemcpyDeviceToHost));
+    size_t bad = 0, first = guard, last = 0;
+    for (size_t k = 0; k < guard; ++k)
+      if (g[k] != 0xA5) {
+        ++bad;
+        first = std::min(first, k);
+        last = k;
+      }
+    if (bad)
+      fprintf(stderr, "rfd guard: %zu bytes written past the workspace (offsets %zu..%zu of %zu)\n",
+              bad, first, last, guard);
+  }
   if (hmisc[1] >= kCheckBase)
     return fail(RFD_ERR_INTERNAL, "device self-check " + std::to_string(hmisc[1] - kCheckBase) +
                                       " failed (boundary ring index out of range)");
@@ -1590,6 +1806,30 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     fprintf(stderr, "rfd trace lag split (ns, %zu strips): input->tile %.0f  tile->steps %.0f  "
             "steps->next input %.0f  next input->output %.0f\n",
             l1.size(), med(l1), med(l2), med(l3), med(l4));
+    // batch: when pairs ended their searches (ms after the first), and the last ones
+    if (npairs > 1) {
+      std::vector<std::pair<unsigned long long, int64_t>> fin;
+      for (int64_t p = 0; p < npairs; ++p)
+        if (hs[p].t_done) fin.push_back({hs[p].t_done, p});
+      std::sort(fin.begin(), fin.end());
+      if (!fin.empty()) {
+        const double t0 = (double)fin.front().first;
+        auto at = [&](double q) {
+          return ((double)fin[std::min(fin.size() - 1, (size_t)(q * fin.size()))].first - t0) / 1e6;
+        };
+        fprintf(stderr, "rfd search ends (ms after the first, %zu pairs): 50%% %.1f  90%% %.1f  "
+                "97%% %.1f  99%% %.1f  last %.1f\n", fin.size(), at(0.5), at(0.9), at(0.97),
+                at(0.99), ((double)fin.back().first - t0) / 1e6);
+        for (size_t k = fin.size() > 12 ? fin.size() - 12 : 0; k < fin.size(); ++k) {
+          const int64_t p = fin[k].second;
+          const PairDesc& Dt = ((const PairDesc*)(hbase + L.h_tdescs))[p];
+          fprintf(stderr, "  pair %lld: %d x %d (team strips %d%s), probes %d, ended %.1f ms\n",
+                  (long long)p, hd[p].n1, hd[p].n2, (Dt.n1 - 1 + 31) / 32,
+                  Dt.tr ? ", transposed" : "", hs[p].srch.probes,
+                  ((double)fin[k].first - t0) / 1e6);
+        }
+      }
+    }
   }
   if (ctx->timing) {
     float a = 0.f, b = 0.f, c = 0.f;

@@ -431,7 +431,11 @@ int32_t rfd_model_destroy(rfd_model* md) {
 int32_t rfd_model_set_params(rfd_model* md, const float* params, int64_t n) {
   if (!md || !params || n != (int64_t)kParams) return mfail(RFD_ERR_ARG, "parameter count");
   MLP_CUDA(cudaSetDevice(md->device));
-  MLP_CUDA(cudaMemcpy(md->w, params, sizeof(float) * kParams, cudaMemcpyHostToDevice));
+  // On the model's stream, ahead of the BF16 conversion: a plain cudaMemcpy from pageable
+  // memory may return before its DMA lands, and the model's stream (non-blocking) does not
+  // wait for it, so the conversion could read stale parameters.
+  MLP_CUDA(cudaMemcpyAsync(md->w, params, sizeof(float) * kParams, cudaMemcpyHostToDevice,
+                           md->stream));
   to_bf16_kernel<<<256, 256, 0, md->stream>>>(md->w, md->wh, kParams);
   MLP_CUDA(cudaMemsetAsync(md->m, 0, sizeof(float) * kParams, md->stream));
   MLP_CUDA(cudaMemsetAsync(md->v, 0, sizeof(float) * kParams, md->stream));
@@ -443,8 +447,9 @@ int32_t rfd_model_set_params(rfd_model* md, const float* params, int64_t n) {
 int32_t rfd_model_get_params(rfd_model* md, float* params, int64_t n) {
   if (!md || !params || n != (int64_t)kParams) return mfail(RFD_ERR_ARG, "parameter count");
   MLP_CUDA(cudaSetDevice(md->device));
+  MLP_CUDA(cudaMemcpyAsync(params, md->w, sizeof(float) * kParams, cudaMemcpyDeviceToHost,
+                           md->stream));
   MLP_CUDA(cudaStreamSynchronize(md->stream));
-  MLP_CUDA(cudaMemcpy(params, md->w, sizeof(float) * kParams, cudaMemcpyDeviceToHost));
   return RFD_OK;
 }
 
