@@ -71,8 +71,9 @@ def parse():
                     help="profiling case: one batched call (one probe) on the first N pairs of "
                          "the uneven batch, then exit (no JSON line)")
     ap.add_argument("--profile-search", type=int, default=0, metavar="N",
-                    help="profiling case: one batched call of the learned form (every probe) on "
-                         "the first N pairs of the uneven batch, then exit (no JSON line)")
+                    help="profiling case: one batched call of the learned form (every probe, "
+                         "k-ary rounds) on the first N pairs of the uneven batch, then exit (no "
+                         "JSON line)")
     ap.add_argument("--profile-bounds", type=int, default=0, metavar="N",
                     help="profiling case: N calls of the exact bounds (DFD, then VE-FD pruned by "
                          "it) on the long pair of --points points, then exit (no JSON line)")
@@ -475,7 +476,7 @@ def main():
         pairs = batch_pairs()[: args.profile_search]
         ctx = rfd.Context(0)
         ctx.distance_batch([p for p, _ in pairs], [q for _, q in pairs], precise=True,
-                           model=rfd.Model.pretrained(0))
+                           model=rfd.Model.pretrained(0), search_arity=ARITY)
         ctx.close()
         return
 
@@ -506,6 +507,10 @@ def main():
 
     def step_plain():
         return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True)
+
+    def step_plain_kary():
+        return ctx.distance_device(dP.data_ptr(), n1, dQ.data_ptr(), n2, d, precise=True,
+                                   search_arity=ARITY)
 
     def timed(fn, k):
         times, res = [], None
@@ -563,6 +568,11 @@ def main():
     pphase = ctx.phase_times(enable=0)
     rel = abs(pres["distance"] - res["distance"]) / pres["distance"]
     assert rel <= 1e-9, f"learned and plain results differ by {rel:.3g}"
+    # the plain method with k-ary rounds: ARITY radii per launch round
+    step_plain_kary()
+    ktimes, kres = timed(step_plain_kary, args.plain_steps)
+    krel = abs(kres["distance"] - pres["distance"]) / pres["distance"]
+    assert krel <= 1e-9, f"k-ary and bisection results differ by {krel:.3g}"
 
     peak = ctx.fp64_peak()
     calls = max(phases["calls"], 1)
@@ -612,7 +622,12 @@ def main():
         "plain": {"solves_per_s": args.plain_steps / (sum(ptimes) * 1e-3),
                   "ms_per_solve": sum(ptimes) / args.plain_steps, "probes": pres["probes"],
                   "phase_ms": {k: pphase[k + "_ms"] / pcalls for k in ("dfd", "vefd", "search")},
-                  "rel_dev_vs_learned": rel},
+                  "rel_dev_vs_learned": rel,
+                  "kary": {"search_arity": ARITY,
+                           "solves_per_s": args.plain_steps / (sum(ktimes) * 1e-3),
+                           "ms_per_solve": sum(ktimes) / args.plain_steps,
+                           "decisions": kres["probes"], "flags": kres["flags"],
+                           "rel_dev_vs_bisection": krel}},
         "free_space_cells_per_s": {
             "nominal": res["cells_nominal"] / (ph_ms["search"] * 1e-3),
             "evaluated": res["cells_evaluated"] / (ph_ms["search"] * 1e-3),

@@ -119,10 +119,11 @@ typedef struct rfd_options {
                                certifies the fused intervals only: it needs RFD_FORMULA_FUSED. */
   int32_t search_arity;     /* 0 or 1 (default): every probe is one decision at the bisection's
                                midpoint (the reference's search, src/frechet.cpp:36-63).  K in
-                               [2, RFD_MAX_ARITY] (batches, rfd_distance_batch): the pairs whose
-                               probe chains are longest (up to RFD_ARITY_PAIRS per call) get K - 1
-                               extra decision workspaces, and once few pairs remain (at most the
-                               teams / (2K), or RFD_ARITY_GATE) each of their bisection rounds
+                               [2, RFD_MAX_ARITY]: the pairs whose probe chains are longest (up to
+                               RFD_ARITY_PAIRS per call, within a quarter of the free device
+                               memory) get K - 1 extra decision workspaces, and once few pairs
+                               remain (at most the teams / (2K), or RFD_ARITY_GATE; a single
+                               pair always) each of their bisection rounds
                                decides K radii at once, splitting the bracket into K + 1 parts
                                (about log2(K + 1) halvings per round instead of one).  Only the
                                probe sequence changes: every decision is the same function of its

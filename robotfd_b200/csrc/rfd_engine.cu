@@ -487,16 +487,19 @@ __device__ PairState* kary_member(const WaveArgs& wa, PairState* g, int m) {
   return m == 0 ? g : wa.st + g->kary_base + (m - 1);
 }
 
-// Starts pair p's next probe (phase PH_SEARCH, split set by next_probe): one decision, or a
-// k-ary round.  One thread.
-__device__ void start_next(const WaveArgs& wa, PairState* g, int p, int S) {
+// Sets up pair g's next probe (phase PH_SEARCH, split set by next_probe): a k-ary round's
+// members get their radii and states; returns the decisions of the round (1: one decision at
+// the split).  Queues nothing: a launch round takes the members' strips from its item list,
+// the continuous search queues them (start_next).  One thread.
+__device__ int kary_arm(const WaveArgs& wa, PairState* g) {
   int n = 1;
   if (g->kary_cap > 0 && wa.kary_k >= 2 && g->srch.mode == SM_BISECT &&
       ld_volatile(wa.active_pairs) <= wa.kary_gate) {
     // the widest round whose decisions still close the gap within the probe cap: halvings
-    // left h, rounds of n radii take ceil(h / log2(n + 1)) of them
+    // left h (against the stop width at lb, which the final ub cannot undercut), rounds of n
+    // radii take ceil(h / log2(n + 1)) of them
     const Search& q = g->srch;
-    const double w = q.stop_mode == 0 ? q.tol : q.tol * q.ub;
+    const double w = q.stop_mode == 0 ? q.tol : q.tol * q.lb;
     const double h = w > 0.0 ? ceil(log2(fmax((q.ub - q.lb) / w, 1.0))) : 64.0;
     const int budget = q.max_probes - q.probes;
     for (n = min(wa.kary_k, g->kary_cap + 1); n >= 2; --n)
@@ -513,10 +516,7 @@ __device__ void start_next(const WaveArgs& wa, PairState* g, int p, int S) {
       if (x > prev && x < g->srch.ub) r[m++] = prev = x;
     }
   }
-  if (m < 2) {
-    start_probe(wa, g, p, S);
-    return;
-  }
+  if (m < 2) return 1;
   g->kary_n = m;
   g->kary_left = m;
   for (int k = 0; k < m; ++k) {
@@ -528,13 +528,29 @@ __device__ void start_next(const WaveArgs& wa, PairState* g, int p, int S) {
     ms->active = 1;
   }
   __threadfence();
-  for (int k = 0; k < m; ++k)
+  return m;
+}
+
+// Continuous search: queues the first strips of every decision of pair p's armed probe.
+__device__ void start_armed(const WaveArgs& wa, PairState* g, int p, int S) {
+  if (g->kary_n < 2) {
+    start_probe(wa, g, p, S);
+    return;
+  }
+  for (int k = 0; k < g->kary_n; ++k)
     start_probe(wa, kary_member(wa, g, k), k == 0 ? p : g->kary_base + (k - 1), S);
 }
 
-// A decision of a k-ary round ended (its boundary words are cleared); the round's last one
-// combines the outcomes and starts the pair's next probe.  One thread.
-__device__ void kary_done(const WaveArgs& wa, PairState* ms, int S) {
+// Continuous search: arms and starts pair p's next probe.  One thread.
+__device__ void start_next(const WaveArgs& wa, PairState* g, int p, int S) {
+  kary_arm(wa, g);
+  start_armed(wa, g, p, S);
+}
+
+// A decision of a k-ary round ended (in the continuous search, its boundary words are cleared);
+// the round's last one combines the outcomes and arms the pair's next probe, and in the
+// continuous search (queue) starts it.  One thread.
+__device__ void kary_done(const WaveArgs& wa, PairState* ms, int S, bool queue) {
   const int p = ms->kary_real;
   PairState* g = wa.st + p;
   __threadfence();
@@ -562,7 +578,10 @@ __device__ void kary_done(const WaveArgs& wa, PairState* ms, int S) {
   g->srch.probes += n;
   g->kary_n = 0;
   next_probe(g, wa.active_pairs);
-  if (g->phase == PH_SEARCH && g->active) start_next(wa, g, p, S);
+  if (g->phase == PH_SEARCH && g->active) {
+    if (queue) start_next(wa, g, p, S);
+    else kary_arm(wa, g);
+  }
 }
 
 // Continuous search: the first strips of every pair in the search phase.
@@ -570,7 +589,7 @@ __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, i
                                          WaveArgs wa) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
     if (st[p].phase != PH_SEARCH || !st[p].active) continue;
-    start_probe(wa, st + p, p, (pairs[p].n1 - 1 + 31) >> 5);
+    start_armed(wa, st + p, p, (pairs[p].n1 - 1 + 31) >> 5);
   }
 }
 
@@ -672,6 +691,11 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
           __threadfence();
           if (dyn && st->phase == PH_SEARCH && st->active) sh->push = 1;
           else if (dyn && st->phase == PH_KWAIT) sh->push = 2;
+          // launch rounds: the next launch runs what is armed here (its fill resets the rows)
+          else if (KIND == K_DEC && !dyn && st->phase == PH_KWAIT) kary_done(wa, st, S, false);
+          else if (KIND == K_DEC && !dyn && st->phase == PH_SEARCH && st->active &&
+                   st->kary_cap > 0)
+            kary_arm(wa, st);
         }
       }
     }
@@ -690,7 +714,7 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
       __syncthreads();
       if (threadIdx.x == 0) {
         if (sh->push == 1) start_next(wa, st, p, S);
-        else kary_done(wa, st, S);
+        else kary_done(wa, st, S, true);
       }
     }
   }
@@ -1137,10 +1161,6 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     ntitems += St;
   }
   if (nitems > INT32_MAX / 2) return fail(RFD_ERR_LIMIT, "too many strips");
-  L.nitems = (int)nitems;
-  L.ntitems = (int)ntitems;
-  L.items = take(sizeof(int2) * nitems);
-  L.titems = take(sizeof(int2) * ntitems);
   // Continuous search: a queue slot for every strip of every probe
   // (at most 512 MB; past that, and for the solo strips, one launch per probe round)
   int64_t dyn_cap = 0;
@@ -1153,11 +1173,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // k-ary rounds (rfd_options.search_arity = K): the pairs whose probe chains are longest get
   // K - 1 member decisions each (descriptor, state and boundary rows of their own, after the
   // pairs' in the same arrays).  A decision's chain is about max(strips x 7 us, 32-column
-  // chunks x 3 us) on a B200; members of more than 256 MB are not given.
-  const int karity = (dyn_cap && mode == MODE_DISTANCE && o.search_arity >= 2)
-                         ? std::min<int>(o.search_arity, RFD_MAX_ARITY) : 0;
+  // chunks x 3 us) on a B200.  The members of all pairs together use at most a quarter of
+  // the device memory that is free or already the context's; a pair whose members would
+  // exceed what is left gets none.
+  const int karity = (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo &&
+                      o.search_arity >= 2) ? std::min<int>(o.search_arity, RFD_MAX_ARITY) : 0;
   std::vector<int64_t> kpairs;
   if (karity) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = 0;
+    }
+    double room = 0.25 * ((double)free_b + (double)ctx->dws_size);
+    std::vector<double> mbytes(npairs, 0.0);
     std::vector<std::pair<double, int64_t>> est;
     for (int64_t p = 0; p < npairs; ++p) {
       if (n1s[p] < 2 || n2s[p] < 2) continue;
@@ -1165,19 +1194,29 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       const double bytes = 8.0 * (double)std::max<int64_t>(St - 1, 1) * (double)align_up((size_t)C, 32) +
                            4.0 * (double)std::max<int64_t>(St - 1, 1) * (double)(C / 32 + 64) +
                            (double)sizeof(Prog) * (double)St;
-      if (bytes > 256.0 * (1 << 20)) continue;
+      mbytes[p] = bytes * (karity - 1);
       est.push_back({std::max(7.0 * (double)St, 3.0 * (double)((C + 31) / 32)), p});
     }
     std::stable_sort(est.begin(), est.end(), [](const std::pair<double, int64_t>& a,
                                                 const std::pair<double, int64_t>& b) {
       return a.first > b.first;
     });
-    for (size_t k = 0; k < est.size() && k < (size_t)RFD_ARITY_PAIRS; ++k)
+    for (size_t k = 0; k < est.size() && kpairs.size() < (size_t)RFD_ARITY_PAIRS; ++k) {
+      if (mbytes[est[k].second] > room) continue;
+      room -= mbytes[est[k].second];
       kpairs.push_back(est[k].second);
+    }
   }
   const int64_t nmem = (int64_t)kpairs.size() * (karity > 1 ? karity - 1 : 0);
   const int64_t nst = npairs + nmem;  // descriptors and states: the pairs', then the members'
   auto mpair = [&](int64_t v) { return kpairs[v / (karity - 1)]; };
+  // the members' strips join the team item list, interleaved with their pair's
+  for (int64_t v = 0; v < nmem; ++v) ntitems += (trows(mpair(v)) + 31) / 32;
+  if (ntitems > INT32_MAX / 2) return fail(RFD_ERR_LIMIT, "too many strips");
+  L.nitems = (int)nitems;
+  L.ntitems = (int)ntitems;
+  L.items = take(sizeof(int2) * nitems);
+  L.titems = take(sizeof(int2) * ntitems);
   L.tdescs = take(sizeof(PairDesc) * nst);
   L.states = take(sizeof(PairState) * nst);
   // ticket counters: DFD, two VE-FD, probe rounds (+1 for a decision), the continuous
@@ -1406,7 +1445,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     for (int64_t sidx = 0; sidx < maxSt; ++sidx)
       for (int64_t q = 0; q < npairs; ++q) {
         const int p = order[q];
-        if (sidx < (trows(p) + 31) / 32) ht[k++] = make_int2(p, (int)sidx);
+        if (sidx < (trows(p) + 31) / 32) {
+          ht[k++] = make_int2(p, (int)sidx);
+          for (int m = 0; m < hs[p].kary_cap; ++m)
+            ht[k++] = make_int2(hs[p].kary_base + m, (int)sidx);
+        }
       }
   }
 
@@ -1537,10 +1580,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     int li = 0;
     // boundary rows of the pairs about to run `ph` back to "not yet written" (team strips)
     // (at least 32 blocks per pair: late probe rounds leave a few large pairs active)
-    const int fill_gy = (int)std::min<int64_t>(npairs, 8 * ctx->num_sms);
+    const int fill_gy = (int)std::min<int64_t>(nst, 8 * ctx->num_sms);
     const int fill_gx = std::max(32, 8 * ctx->num_sms / fill_gy);
     auto fill = [&](int ph) {
-      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dt, ds, (int)npairs, ph, wa.gate,
+      bnd_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(dt, ds, (int)nst, ph, wa.gate,
                                                                wa.active_pairs, wa.gate_min);
       ++launches;
     };
@@ -1627,6 +1670,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
     if (ctx->timing) RFD_CUDA(record(2));
     const int nprobe = mode == MODE_DECIDE ? 1 : max_probes;
+    wa.kary_k = karity;
+    wa.kary_gate = kary_gate;
     if (dyn_cap) {
       // Probe rounds as single launches while many pairs are active (the rounds then keep
       // every team busy, and a launch interleaves all pairs' strips), each skipped once
@@ -1651,8 +1696,6 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       wa.dyn_cap = dyn_cap;
       wa.window = ctx->search_window;
       wa.window_teams = ctx->team_grid[K_DEC];
-      wa.kary_k = karity;
-      wa.kary_gate = kary_gate;
       const int nstatic = wa.nitems;
       wa.nitems = 0;  // every strip comes from the queue
       fill(PH_SEARCH);
@@ -1714,6 +1757,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     mix(n2s, sizeof(int64_t) * npairs);
     mix(dims, sizeof(int32_t) * npairs);
     mix(formula.data(), sizeof(int) * formula.size());
+    if (!kpairs.empty()) mix(kpairs.data(), sizeof(int64_t) * kpairs.size());
   }
   if (use_graph && ctx->gexec && ctx->gkey == key) {
     RFD_CUDA(cudaGraphLaunch(ctx->gexec, st));

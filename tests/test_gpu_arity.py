@@ -82,10 +82,22 @@ def test_kary_default_gate_and_graph_replay(ctx, built):
         assert abs(x["distance"] - z["distance"]) <= 2 * REL * z["ub"]
 
 
-def test_single_pair_calls_ignore_arity(ctx, built):
-    """A single-pair call runs probe rounds as launches: search_arity leaves it bit for bit."""
+@pytest.mark.parametrize("precise", [True, False])
+def test_single_pair_kary_rounds(ctx, built, precise):
+    """A single-pair call runs its probe rounds as launches; with search_arity each launch
+    decides K radii of the pair (its members' strips interleaved in the launch's items).
+    Reference mode (precise=False) keeps its absolute FLT_EPSILON stop."""
     P, Q = built.gen_pair(1, 3, 3000, 2800, 100.0, 0.1, 23, 0)
-    a = ctx.distance(P, Q, precise=True)
-    b = ctx.distance(P, Q, precise=True, search_arity=4)
-    for k in ("distance", "lb", "ub", "probes"):
-        assert a[k] == b[k]
+    a = ctx.distance(P, Q, precise=precise)
+    b = ctx.distance(P, Q, precise=precise, search_arity=4)
+    assert (b["dfd"], b["vefd"]) == (a["dfd"], a["vefd"])
+    assert not b["flags"] & SF_MAX_PROBES
+    tol = REL * b["ub"] if precise else float(np.finfo(np.float32).eps)
+    assert b["lb"] <= b["distance"] <= b["ub"] and b["ub"] - b["lb"] <= tol
+    assert abs(b["distance"] - a["distance"]) <= 2 * (REL * a["ub"] if precise else tol)
+    assert b["probes"] > a["probes"]  # more decisions, in fewer rounds
+    t = oracle.max_threads()
+    if b["ub"] < b["dfd"]:
+        assert oracle.decide(P, Q, b["ub"], threads=t)[0]
+    if b["lb"] > b["vefd"]:
+        assert not oracle.decide(P, Q, b["lb"], threads=t)[0]
