@@ -275,9 +275,10 @@ def batch_leg(ctx, model, timed, sample=128, dist=None):
     if dist is not None:
         import torch
         from robotfd_b200 import shard
-        shard.distance_batch_sharded(ctx, Ps[:256], Qs[:256], precise=True, model=model)  # warm
+        shard.distance_batch_sharded(ctx, Ps[:256], Qs[:256], precise=True, model=model,
+                                     search_arity=ARITY)  # warm
         t_s, res = timed(lambda: shard.distance_batch_sharded(ctx, Ps, Qs, precise=True,
-                                                              model=model), 2)
+                                                              model=model, search_arity=ARITY), 2)
         t = torch.tensor([statistics.median(t_s)], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return {
