@@ -70,11 +70,13 @@ struct PairDesc {
   const double* Q;        // curve 2, [n2][d]
   const double2* rowc;    // [n1-1]: (|p_{i+1}-p_i|^2, 0.5 / that)
   const double2* colrec;  // [n2-1][RECW(d)]: q_j, q_{j+1}, (|q_{j+1}-q_j|^2, 0.5 / that)
-  double* bnd;            // boundary rows: [S-1][cstride] (team strips), [ring][cstride] (DFD)
-  unsigned int* tags;     // [S-1][tstride] epoch tag of every live chunk (team strips)
+  double* bnd;            // boundary rows: [ring][cstride] (team strips and DFD)
+  unsigned int* tags;     // [ring][tstride] epoch tag of every live chunk (team strips)
   Prog* prog;             // [S]
   unsigned long long* slots;  // [S] cleared count of every DFD strip (see Boundary ring)
-  int ring;                   // rows of the DFD ring (>= 1; rows never wrap when >= S-1)
+  // rows of the boundary ring (>= 1; rows never wrap when >= S-1).  DFD strips: see Boundary
+  // ring.  Team strips: S - 1 (one row each), or the rows of a launch window plus one.
+  int ring;
   // tr: the team strips of a pair whose first curve is the longer run on the transposed
   // grid (rows = curve 2), whose free intervals are the same values (the interval of an edge
   // is the same function of its point and segment in either orientation) with the roles of

@@ -404,6 +404,31 @@ __global__ void member_fill_kernel(const PairDesc* pairs, int first, int count) 
   }
 }
 
+// Launch windows of the team strips (O(n+m) boundary memory): strips s0 .. s0+count-1 of
+// every pair about to run `phase` write ring rows s % ring; those rows go back to "not yet
+// written" and their tags to 0 (no epoch is 0) before the window's launch.  The ring has at
+// least count + 1 rows, so the row the window's first strip reads - written by strip s0 - 1
+// in the previous window, which has ended - is not among them.  Pairs over grid rows (y),
+// each pair's rows over grid columns (x).
+__global__ void team_window_fill_kernel(const PairDesc* pairs, const PairState* st, int npairs,
+                                        int phase, int s0, int count) {
+  for (int p = blockIdx.y; p < npairs; p += gridDim.y) {
+    if (st[p].phase != phase || !st[p].active) continue;
+    const PairDesc pd = pairs[p];
+    const int S = (pd.n1 - 1 + 31) / 32;
+    const int s1 = min(s0 + count, S - 1);  // strips with a consumer write a row
+    for (int s = s0 + (int)blockIdx.x; s < s1; s += gridDim.x) {
+      const long long r = s % pd.ring;
+      // cstride is a multiple of 32 doubles and bnd 256-byte aligned: 16-byte stores
+      ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd + r * pd.cstride);
+      for (long long k = threadIdx.x; k < pd.cstride / 2; k += blockDim.x)
+        b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
+      unsigned* t = pd.tags + r * pd.tstride;
+      for (long long k = threadIdx.x; k < pd.tstride; k += blockDim.x) t[k] = 0u;
+    }
+  }
+}
+
 // Dense DFD strips of 32*K rows (rfd_dfd.cuh), same in-order ticket scheme as wave_kernel
 // over the (pair, 32-row strip) item list: item (p, s) is strip s of 32*K rows, items past
 // the pair's last tall strip are skipped.
@@ -865,6 +890,9 @@ struct rfd_context {
   // rows of the DFD strips' boundary ring per pair (RFD_DFD_RING_ROWS, at least 2; see
   // "Boundary ring" in rfd_device.cuh)
   int dfd_ring_rows = kDfdRingRows;
+  // rows of the VE-FD and decision strips' boundary ring (RFD_TEAM_RING_ROWS, at least 2):
+  // 0 keeps one row per strip unless a lone pair's rows do not fit (launch windows, run_batch)
+  int team_ring_rows = 0;
   void* dws = nullptr;
   size_t dws_size = 0;
   void* hws = nullptr;
@@ -1161,10 +1189,51 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     ntitems += St;
   }
   if (nitems > INT32_MAX / 2) return fail(RFD_ERR_LIMIT, "too many strips");
+  // Launch windows of the team strips (O(n+m) boundary memory).  One boundary row per 32-row
+  // strip takes about n1 n2 / 4 bytes (250 GB for two curves of 10^6 points).  When a lone
+  // pair's workspace does not fit in the memory this context may use (3/4 of what is free and
+  // its own workspace, or RFD_BATCH_BUDGET bytes), or RFD_TEAM_RING_ROWS = R asks for it, the
+  // VE-FD and decision strips run in launch windows of W consecutive strips: strip s writes
+  // ring row s % (W + 1), a window's rows are reset right before its launch, and the next
+  // window starts once it has ended.  The boundary then takes W + 1 rows whatever the curves'
+  // lengths; W is the most the budget holds, at most 4096 strips (R - 1 when forced): a window
+  // of 4096 strips keeps every team busy, and a window's end costs one strip's drain (tens of
+  // microseconds in a pruned band).  Results are bit-identical:
+  // the same strips compute the same values and hand over the same rows.  The continuous
+  // search and the k-ary members, which keep every strip's row at once, are off (one launch
+  // round per probe, one launch per window).
+  int64_t twin = 0;  // team strips per launch window; 0: every strip in one launch
+  if (!ctx->solo) {
+    if (ctx->team_ring_rows >= 2) {
+      twin = ctx->team_ring_rows - 1;
+    } else if (npairs == 1 && n1s[0] >= 2 && n2s[0] >= 2) {
+      const int64_t St = (trows(0) - 1 + 31) / 32;
+      const double full = pair_workspace_bytes(ctx, n1s[0], n2s[0], dims[0], ck);
+      double budget = 0.0;
+      if (const char* e = getenv("RFD_BATCH_BUDGET")) budget = atof(e);
+      if (!(budget > 0.0)) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+          cudaGetLastError();
+          fr = 0;
+        }
+        budget = 0.75 * ((double)fr + (double)ctx->dws_size);
+      }
+      if (St > 2 && full > budget) {
+        // a team row and its tags, as pair_workspace_bytes counts them
+        const double row = 8.0 * (double)(tcols(0) + 32) + 4.0 * (double)(tcols(0) / 32 + 64);
+        const double rows = std::floor((budget - (full - (double)(St - 1) * row)) / row);
+        // fewer than 2 rows: not even a window of one strip fits (the allocation reports it)
+        twin = rows >= 2.0 ? std::min<int64_t>({St - 2, (int64_t)rows - 1, (int64_t)4096}) : 0;
+      }
+    }
+    if (twin >= maxSt) twin = 0;  // one window holds every strip: nothing to gain
+  }
+  const int64_t nwin = twin ? (maxSt + twin - 1) / twin : 0;
   // Continuous search: a queue slot for every strip of every probe
   // (at most 512 MB; past that, and for the solo strips, one launch per probe round)
   int64_t dyn_cap = 0;
-  if (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo && !ctx->lockstep) {
+  if (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo && !ctx->lockstep && !twin) {
     for (int64_t p = 0; p < npairs; ++p)
       dyn_cap += (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32 * max_probes;
     if (dyn_cap * (int64_t)sizeof(unsigned long long) > ((int64_t)512 << 20)) dyn_cap = 0;
@@ -1176,7 +1245,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // chunks x 3 us) on a B200.  The members of all pairs together use at most a quarter of
   // the device memory that is free or already the context's; a pair whose members would
   // exceed what is left gets none.
-  const int karity = (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo &&
+  const int karity = (mode == MODE_DISTANCE && max_probes > 1 && !ctx->solo && !twin &&
                       o.search_arity >= 2) ? std::min<int>(o.search_arity, RFD_MAX_ARITY) : 0;
   std::vector<int64_t> kpairs;
   if (karity) {
@@ -1222,8 +1291,11 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // ticket counters: DFD, two VE-FD, probe rounds (+1 for a decision), the continuous
   // search's ticket and queue tail; then a gate word per probe round
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
+  // launch windows: a ticket counter per window of every VE-FD phase and probe round
+  const int64_t wbase = L.nlaunch + max_probes + 1;
+  const int64_t wtickets = nwin * (2 + std::max(max_probes, 1));
   L.zero_begin = off;
-  L.counters = take(sizeof(unsigned) * (L.nlaunch + max_probes + 1));
+  L.counters = take(sizeof(unsigned) * (wbase + wtickets));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + kTraceW * kTrace));
   L.error = take(sizeof(int));
   for (int64_t p = 0; p < npairs; ++p) {
@@ -1231,7 +1303,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // at least 32 point rows (the strip height the autotuner may pick); the coarse pair's DFD
     const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
     // team strips hand rows over through one row per strip (S - 1 rows)
-    L.ring_t[p] = ring_of(St, INT32_MAX);
+    L.ring_t[p] = ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
     L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
     L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
                       ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
@@ -1433,6 +1505,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       hs[p].kary_cap = karity - 1;
     }
   }
+  std::vector<int> wstart(nwin + 1, 0);  // launch windows: first team item of each
   {
     int64_t k = 0;
     for (int64_t sidx = 0; sidx < maxS; ++sidx)
@@ -1442,7 +1515,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       }
     int2* ht = (int2*)(hbase + L.h_titems);
     k = 0;
-    for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+    for (int64_t sidx = 0; sidx < maxSt; ++sidx) {
+      if (twin && sidx % twin == 0) wstart[sidx / twin] = (int)k;  // strip-major: windows are ranges
       for (int64_t q = 0; q < npairs; ++q) {
         const int p = order[q];
         if (sidx < (trows(p) + 31) / 32) {
@@ -1451,6 +1525,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
             ht[k++] = make_int2(hs[p].kary_base + m, (int)sidx);
         }
       }
+    }
+    if (twin) wstart[nwin] = (int)k;
   }
 
   if (!on_device) {
@@ -1587,6 +1663,29 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                                                                wa.active_pairs, wa.gate_min);
       ++launches;
     };
+    // One VE-FD phase or probe round of the team strips: the rows reset and one launch, or
+    // with launch windows a reset and a launch per window, in strip order (each window's
+    // items are a range of the strip-major item list).
+    unsigned* wtick = counters + wbase;
+    auto team_round = [&](auto kind, int ph) {
+      constexpr int KIND = decltype(kind)::value;
+      if (!twin) {
+        fill(ph);
+        launch_team<KIND>(ctx, wa, st);
+        return;
+      }
+      WaveArgs w = wa;
+      const int2* items0 = (const int2*)(dbase + L.titems);
+      for (int64_t g = 0; g < nwin; ++g) {
+        team_window_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(
+            dt, ds, (int)nst, ph, (int)(g * twin), (int)twin);
+        w.items = items0 + wstart[g];
+        w.nitems = wstart[g + 1] - wstart[g];
+        w.ticket = wtick++;
+        launch_team<KIND>(ctx, w, st);
+      }
+      launches += (int)(2 * nwin - 1);  // the caller counts one team launch
+    };
     if (mode != MODE_DECIDE) {
       wa.phase = PH_DFD;
       wa.ticket = counters + li++;
@@ -1645,8 +1744,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         if (ctx->solo) {
           wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
         } else {
-          fill(ph);
-          launch_team<K_VEFD>(ctx, wa, st);
+          team_round(std::integral_constant<int, K_VEFD>{}, ph);
         }
         RFD_CUDA(cudaGetLastError());
       }
@@ -1721,8 +1819,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       if (ctx->solo) {
         wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
       } else {
-        fill(PH_SEARCH);
-        launch_team<K_DEC>(ctx, wa, st);
+        team_round(std::integral_constant<int, K_DEC>{}, PH_SEARCH);
       }
       RFD_CUDA(cudaGetLastError());
       ++launches;
@@ -1746,7 +1843,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
                          ctx->search_switch, ctx->search_window, ctx->team_warps,
                          (int)(ctx->spin_cycles >> 32),
-                         (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate};
+                         (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate, (int)twin};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));
@@ -2050,6 +2147,7 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     const char* pe = getenv("RFD_PROF");
     c->prof = pe && pe[0] == '1';
     c->dfd_ring_rows = env_rows("RFD_DFD_RING_ROWS", kDfdRingRows);
+    c->team_ring_rows = env_rows("RFD_TEAM_RING_ROWS", 0);
   }
   // wait budget: about 20 s at the maximum SM clock, or RFD_SPIN_CYCLES
   c->spin_default = (long long)prop.clockRate * 1000LL * 20LL;

@@ -295,12 +295,17 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   const bool has_cons = s + 1 < S;
   const bool tr = pd.tr != 0;
 
+  // Strip s writes boundary row s % ring (and its tags).  ring >= S - 1 unless the strips run
+  // in launch windows of ring - 1 strips (rfd_engine.cu, team_window_fill_kernel): a window's
+  // strips then write distinct rows, none of them the row its first strip reads.
+  const int rin = has_prod ? (s - 1) % pd.ring : 0;
+  const int rout = has_cons ? s % pd.ring : 0;
   Prog* in_prog = has_prod ? pd.prog + (s - 1) : nullptr;
   Prog* out_prog = has_cons ? pd.prog + s : nullptr;
-  const double* in_bnd = has_prod ? pd.bnd + (size_t)(s - 1) * pd.cstride : nullptr;
-  double* out_bnd = has_cons ? pd.bnd + (size_t)s * pd.cstride : nullptr;
-  const unsigned* in_tags = has_prod ? pd.tags + (size_t)(s - 1) * pd.tstride : nullptr;
-  unsigned* out_tags = has_cons ? pd.tags + (size_t)s * pd.tstride : nullptr;
+  const double* in_bnd = has_prod ? pd.bnd + (size_t)rin * pd.cstride : nullptr;
+  double* out_bnd = has_cons ? pd.bnd + (size_t)rout * pd.cstride : nullptr;
+  const unsigned* in_tags = has_prod ? pd.tags + (size_t)rin * pd.tstride : nullptr;
+  unsigned* out_tags = has_cons ? pd.tags + (size_t)rout * pd.tstride : nullptr;
 
   int status = 0;
   Waiter wt;
