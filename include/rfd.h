@@ -229,7 +229,8 @@ int32_t rfd_autotune_search(rfd_context* ctx, int64_t npairs, const double* cons
    symmetric with a zero diagonal; entry (i, j), i < j, is the distance with curve i as the
    first curve.  results (optional) receives the ncurves (ncurves - 1) / 2 pair results in
    that order.  Pairs go through rfd_distance_batch in chunks whose strip boundary rows
-   (n_i n_j / 4 bytes a pair) stay within budget_bytes (<= 0: 8e9).  opt->bracket must be NULL;
+   (n_i n_j / 4 bytes a pair; a pair that alone exceeds the budget runs in launch windows of
+   O(n_i + n_j) memory) stay within budget_bytes (<= 0: 8e9).  opt->bracket must be NULL;
    the curves of a pair must have equal dims. */
 int32_t rfd_distance_matrix(rfd_context* ctx, int64_t ncurves, const double* const* curves,
                             const int64_t* ns, const int32_t* dims, const rfd_options* opt,

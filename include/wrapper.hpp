@@ -4,8 +4,10 @@
 // decision paths as the reference does: forced, or when the reference's materialised interval
 // arrays would not fit in free device memory, the fused kernel's free intervals; otherwise the
 // materialised path's (they differ in one rounding, rfd.h enum rfd_formula).  Device memory is
-// the same either way: O(n1 + n2) for the curves, records and the DFD's boundary ring, plus
-// about n1 * n2 / 4 bytes of boundary rows for the VE-FD and decision strips.
+// the same either way: O(n1 + n2) for the curves, records and the DFD's boundary ring; the
+// VE-FD and decision strips keep a boundary row per 32 rows (about n1 * n2 / 4 bytes) when that
+// fits, and otherwise run in launch windows whose ring of at most 4097 rows is O(n1 + n2), so
+// any pair whose points fit is solved, as by the reference's oversize path.
 #pragma once
 
 #include "curve.hpp"
