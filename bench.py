@@ -15,6 +15,9 @@ free-space cells per decision.  Inputs are synthetic and seeded (the reference s
           calls, and single-pair plain calls on a sample of it
   mixed_precision : large 3D pairs with coordinates ~1e4, FP32 filter against FP64
           (fraction of decision cells computed in FP64, error against the FP64 path)
+  oversize : two 1,000,000-point 3D spline paths (10^12 cells), whose one-row-per-strip
+          boundary (250 GB) does not fit: the VE-FD and decision strips run in launch windows
+          over an O(n+m) ring; learned form with the coarse bound, host buffers
   roofline : the dominant phase kernel against the measured FP64 FMA peak
   cpu_baseline : the CPU oracle (dense FP64 restatement, OpenMP) on a bounded sample,
                  extrapolated to the plain method's probes on the full pair
@@ -67,6 +70,8 @@ def parse():
     ap.add_argument("--mixed-pairs", type=int, default=2,
                     help="pairs of the mixed-precision workload to solve (0: skip that leg)")
     ap.add_argument("--plain-steps", type=int, default=2, help="timed plain-method solves")
+    ap.add_argument("--oversize-points", type=int, default=1000000,
+                    help="points per curve of the oversize pair (0: skip that leg)")
     ap.add_argument("--profile-batch", type=int, default=0, metavar="N",
                     help="profiling case: one batched call (one probe) on the first N pairs of "
                          "the uneven batch, then exit (no JSON line)")
@@ -454,6 +459,41 @@ def mixed_leg(ctx, model, timed, npairs):
     }
 
 
+def oversize_leg(model, timed, points):
+    """Two 3D spline paths of `points` points each (seed 1, stream 7) in a fresh context: one
+    boundary row per 32-row strip would take about points^2 / 4 bytes, so the VE-FD and
+    decision strips run in launch windows over a ring of at most 4097 rows.  One untimed solve
+    sizes the workspace (its growth is reported), then one timed solve with host buffers."""
+    import torch
+    import robotfd_b200 as rfd
+    P, Q = rfd.gen_pair(1, 3, points, points, 100.0, 0.1, 1, 7)
+    c = rfd.Context(torch.cuda.current_device())
+    c.set_stream(torch.cuda.current_stream().cuda_stream)  # the stream `timed` records on
+    try:
+        free0 = torch.cuda.mem_get_info()[0]
+        kw = dict(precise=True, model=model, coarse_ub=COARSE_UB)
+        c.distance(P, Q, **kw)
+        used = free0 - torch.cuda.mem_get_info()[0]
+        c.phase_times(enable=1)
+        t, r = timed(lambda: c.distance(P, Q, **kw), 1)
+        ph = c.phase_times(enable=0)
+    finally:
+        c.close()
+    rows = min(len(P), len(Q))
+    return {
+        "workload": f"2 x {points:,}-point 3D spline paths (waypoints U[-100,100]^3, seed 1, "
+                    "stream 7); learned form, coarse bound k=6, FD to 2^-33; host buffers",
+        "cells_per_decision": (len(P) - 1) * (len(Q) - 1),
+        "one_row_per_strip_bytes": ((rows - 1 + 31) // 32 - 1) * 8 * (len(Q) + 31) // 32 * 32,
+        "device_bytes_used": used,
+        "ms_per_solve": t[0],
+        "phase_ms": {k: ph[k + "_ms"] for k in ("dfd", "vefd", "search")},
+        "probes": r["probes"],
+        "flags": r["flags"],
+        "bracket": [r["lb"], r["ub"]],
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -664,6 +704,8 @@ def main():
         line["batch"] = batch_leg(ctx, model, timed, dist=dist)
     if args.mixed_pairs > 0 and world == 1:
         line["mixed_precision"] = mixed_leg(ctx, model, timed, args.mixed_pairs)
+    if args.oversize_points > 0 and world == 1:
+        line["oversize"] = oversize_leg(model, timed, args.oversize_points)
     if rank == 0:
         if world == 1:
             probes, src = workload_probes(P, Q, args.points)
