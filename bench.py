@@ -429,25 +429,30 @@ def network_timing(model, n):
 
 def mixed_leg(ctx, model, timed, npairs):
     """The mixed-precision workload (config 4: large 3D spline pairs, coordinates ~1e4):
-    the first npairs pairs in one batched call with the bracket network, FP32 filter against
-    FP64 intervals."""
+    the first npairs pairs in one batched call in the learned form (bracket network, coarse
+    upper bound k = COARSE_UB), FP32 filter against FP64 intervals."""
     import robotfd_b200 as rfd
     pairs = rfd.gen_config(4, npairs=npairs)
     Ps, Qs = [p for p, _ in pairs], [q for _, q in pairs]
+    kw = dict(precise=True, model=model, coarse_ub=COARSE_UB)
     # untimed first call: the context's workspace grows to these sizes once
-    ctx.distance_batch(Ps, Qs, precise=True, model=model)
-    t64, r64 = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model), 1)
+    ctx.distance_batch(Ps, Qs, **kw)
     ctx.phase_times(enable=1)
-    t32, r32 = timed(lambda: ctx.distance_batch(Ps, Qs, precise=True, model=model,
-                                                precision=rfd.RFD_PREC_FP32_FILTER), 1)
+    t64, r64 = timed(lambda: ctx.distance_batch(Ps, Qs, **kw), 1)
+    ph64 = ctx.phase_times(enable=0)
+    ctx.phase_times(enable=1)
+    t32, r32 = timed(lambda: ctx.distance_batch(Ps, Qs, precision=rfd.RFD_PREC_FP32_FILTER,
+                                                **kw), 1)
     ph = ctx.phase_times(enable=0)
     err = max(abs(a["distance"] - b["distance"]) / a["distance"] for a, b in zip(r64, r32))
     ev = sum(r["cells_evaluated"] for r in r32)
     return {
         "workload": f"first {npairs} of 512 3D spline pairs (100k-400k points, waypoints "
-                    "U[-1e4,1e4]^3, seed 5), one batched call, bracket network",
+                    "U[-1e4,1e4]^3, seed 5), one batched call, bracket network, coarse upper "
+                    f"bound k={COARSE_UB}",
         "points": [[len(p), len(q)] for p, q in pairs],
         "ms": {"fp64": sum(t64), "fp32_filter": sum(t32)},
+        "phase_ms_fp64": {k: ph64[k + "_ms"] for k in ("dfd", "vefd", "search")},
         "phase_ms_fp32_filter": {k: ph[k + "_ms"] for k in ("dfd", "vefd", "search")},
         "probes": [r["probes"] for r in r32],
         "decision_cells_evaluated": ev,

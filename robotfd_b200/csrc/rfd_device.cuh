@@ -82,6 +82,11 @@ struct PairDesc {
   // is the same function of its point and segment in either orientation) with the roles of
   // the right and top edges exchanged
   int n1, n2, d, tr;
+  // Meet in the middle (team strips of one pair, run_batch): the forward sweep of a split pair
+  // runs its first `split` strips only; the pair's mirror descriptor (split = -1) sweeps the
+  // rest of the grid from the far corner, its row r being row mrow - r of the pair's grid
+  // (n1 then counts the mirror's rows + 1).  0 for every other descriptor.
+  int split, mrow;
   long long cstride, tstride;
 };
 
@@ -112,6 +117,7 @@ struct PairState {
   int kary_left;  // the pair: decisions of the round still running
   int kary_in;    // this decision belongs to a round
   int kary_reach; // its outcome
+  int corner;     // mirror decision: the far corner lies in the free space (see split_sync_kernel)
 };
 
 template <int D>

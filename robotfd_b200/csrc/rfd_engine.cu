@@ -381,9 +381,12 @@ __global__ void bnd_fill_kernel(const PairDesc* pairs, const PairState* st, int 
     if (st[p].phase != phase || !st[p].active) continue;
     const PairDesc pd = pairs[p];
     const long long S = (pd.n1 - 1 + 31) / 32;
-    if (S < 2) continue;
+    // a split pair's forward and mirror sweeps: every row of the ring (the mirror's last
+    // strip hands a row to the meet kernel)
+    const bool meet = pd.split != 0;
+    if (S < 2 && !meet) continue;
     ulonglong2* b = reinterpret_cast<ulonglong2*>(pd.bnd);
-    const long long n = (S - 1) * pd.cstride / 2;
+    const long long n = (meet ? (long long)pd.ring : S - 1) * pd.cstride / 2;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
       b[k] = make_ulonglong2(kBndEmpty, kBndEmpty);
   }
@@ -629,8 +632,11 @@ __global__ void search_queue_init_kernel(const PairDesc* pairs, PairState* st, i
 // teams.  The CTA whose strip ends a pair's probe clears the boundary words the probe's
 // strips wrote (each strip records its written chunk range), then starts the next probe: a
 // pair starts its next probe as soon as its last one ends, not after every pair's.
-template <int KIND, int NW = kTeamThreads / 32>
-__global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
+// MIR: the mirror halves of split pairs (meet in the middle), a kernel of their own so that
+// the forward kernel's registers stay as they are; it runs beside the forward kernel, on
+// another stream, each on half the teams.
+template <int KIND, int NW = kTeamThreads / 32, bool MIR = false>
+__global__ void __launch_bounds__(NW * 32, NW == 8 ? 2 : 1) team_kernel(WaveArgs wa) {
   constexpr int H = NW - 1;  // helper warps
   extern __shared__ __align__(128) unsigned char team_smem[];
   TeamShared* sh = (TeamShared*)team_smem;
@@ -688,12 +694,13 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
     const PairDesc pd = wa.pairs[p];
     PairState* st = wa.st + p;
     if (warp == 0) {
-      const int status = pd.d == 2 ? team_propagator<KIND, 2>(wa, pd, st, s, sh, tiles, seqP, seqC)
-                                   : team_propagator<KIND, 3>(wa, pd, st, s, sh, tiles, seqP, seqC);
+      const int status =
+          pd.d == 2 ? team_propagator<KIND, 2, MIR>(wa, pd, st, s, sh, tiles, seqP, seqC)
+                    : team_propagator<KIND, 3, MIR>(wa, pd, st, s, sh, tiles, seqP, seqC);
       if (lane == 0) sh->status = status;
     } else {
-      if (pd.d == 2) team_helpers<KIND, 2, H>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
-      else team_helpers<KIND, 3, H>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
+      if (pd.d == 2) team_helpers<KIND, 2, H, MIR>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
+      else team_helpers<KIND, 3, H, MIR>(wa, pd, st, s, sh, tiles, stage, seqH, seqS, warp - 1);
     }
     __syncthreads();
     const int S = (pd.n1 - 1 + 31) >> 5;
@@ -710,7 +717,9 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
         if (dyn && sh->push_req != 2) queue_strips(wa, st, p, S, sh->push_req == 3 ? S : 1);
         __threadfence();
         const int n = atomicAdd(&st->done_count, 1);
-        if (n == S - 1) {
+        // (the halves of a split pair, split != 0, end in split_meet_kernel instead; read
+        // from the descriptor here, not kept in registers across the strip)
+        if (n == S - 1 && !MIR && !ld_volatile(&wa.pairs[p].split)) {
           __threadfence();
           finalize<KIND>(st, pd, wa.active_pairs);
           __threadfence();
@@ -742,6 +751,130 @@ __global__ void __launch_bounds__(NW * 32) team_kernel(WaveArgs wa) {
         else kary_done(wa, st, S, true);
       }
     }
+  }
+}
+
+// ---- meet in the middle (one pair's VE-FD and search decisions)
+//
+// A split pair's forward sweep runs its first k strips (grid rows 0 .. 32k - 1) and its mirror
+// sweep (rfd_team.cuh, mirror_interval) the other rows from the far corner, both in the same
+// launch, each a chain half as long.  Every monotone path crosses the boundary between rows
+// 32k - 1 and 32k exactly once, through one edge b of it; the forward sweep's last strip hands
+// over, for each b, the value entering the rows above and the mirror's last strip the value
+// of the rest of the path through the same edge.  split_meet_kernel combines them:
+//   VE-FD: min over b of max(forward, mirror) - the min-max over all paths, split at the
+//          crossing (the same doubles, combined by exact min and max);
+//   decision: reachable iff for some b the forward reachable part [F, ub] and the co-reachable
+//          part [lb, -M] of edge b meet, F <= -M (exact comparisons of the same doubles).
+// Both equal what the unsplit sweep computes.  The decision's right UB is not formed (the
+// search needs only reachable or not), so rfd_decide never splits.
+
+// The far corner of a split pair's mirror: VE-FD starts from min(w_top, w_right) of the last
+// cell, which the forward sweep's last step adds; the decision from the last cell's right
+// edge (top edge on a transposed grid) when its free interval reaches the corner (upper end
+// 1.0), the condition under which the forward sweep reports reachable.  Same functions and
+// operands as the forward sweep's tile of that cell.  One thread.
+template <int D>
+__device__ void split_corner(const PairDesc& pd, PairState* m, const PairState* g, bool dec) {
+  const int R = pd.n1 - 1, C = pd.n2 - 1;
+  RowData<K_DEC, D> row;
+  row.load(pd, R - 1);
+  ColRec<K_DEC, D> col;
+  load_col<K_DEC, D>(pd, C - 1, col);
+  double qd[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) qd[k] = __dsub_rn(col.qb[k], col.qa[k]);
+  if (!dec) {
+    const double wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
+    const double wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
+    m->seed = dmin(wt, wr);
+  } else {
+    double lo, hi;
+    const bool mat = g->formula == 1;
+    if (pd.tr) free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, g->r2, lo, hi, mat);
+    else free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, g->r2, lo, hi, mat);
+    m->corner = hi == 1.0;
+  }
+}
+
+// Before each team launch of a split pair (descriptor p, mirror m): the mirror follows the
+// pair's running phase - radius, pruning bound, epoch, options - with fresh counters and its
+// far corner set up; idle when the pair does not run the phase.  One thread.
+__global__ void split_sync_kernel(const PairDesc* pairs, PairState* sts, int p, int m, int phase) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const PairState* g = sts + p;
+  PairState* ms = sts + m;
+  const bool run = g->phase == phase && g->active;
+  ms->active = run ? 1 : 0;
+  ms->phase = run ? phase : PH_DONE;
+  if (!run) return;
+  ms->r2 = g->r2;
+  ms->split = g->split;
+  ms->U = g->U;
+  ms->epoch = g->epoch;
+  ms->dense = g->dense;
+  ms->filter = g->filter;
+  ms->formula = g->formula;
+  ms->done_count = 0;
+  ms->dead_from = INT_MAX;
+  const PairDesc pd = pairs[p];
+  const bool dec = phase == PH_SEARCH;
+  if (pd.d == 2) split_corner<2>(pd, ms, g, dec);
+  else split_corner<3>(pd, ms, g, dec);
+  __threadfence();
+}
+
+// After each team launch of a split pair: the meet (see above) gives the phase's result,
+// which then ends the phase as the unsplit sweep's last strip would (finalize).  Unwritten
+// boundary words are NaN (all ones) and fail every comparison, i.e. count as dead.  One CTA.
+template <int KIND>
+__global__ void __launch_bounds__(1024) split_meet_kernel(const PairDesc* pairs, PairState* sts,
+                                                          int p, int m, int phase, const int* error,
+                                                          int* active_pairs) {
+  PairState* g = sts + p;
+  PairState* ms = sts + m;
+  if (ld_volatile(&g->phase) != phase || !ld_volatile(&g->active) || ld_volatile(error)) return;
+  const PairDesc pd = pairs[p], md = pairs[m];
+  const int C = pd.n2 - 1;
+  const int Sm = (md.n1 - 1 + 31) >> 5;
+  const double* F = pd.bnd + (size_t)((pd.split - 1) % pd.ring) * pd.cstride;
+  const double* M = md.bnd + (size_t)((Sm - 1) % md.ring) * md.cstride;
+  double r;
+  if (KIND == K_DEC) {
+    int found = 0;
+    for (int b = threadIdx.x; b < C; b += blockDim.x) {
+      const double f = __ldcg(F + b), mm = __ldcg(M + (C - 1 - b));
+      found |= (f >= 0.0 && mm >= -1.5 && f <= -mm) ? 1 : 0;
+    }
+    r = __syncthreads_or(found) ? 1.0 : -2.0;
+  } else {
+    __shared__ double red[32];
+    const double U = g->U;
+    double v = kFltMax;
+    for (int b = threadIdx.x; b < C; b += blockDim.x) {
+      const double f = __ldcg(F + b), mm = __ldcg(M + (C - 1 - b));
+      if (f <= U && mm <= U) v = dmin(v, dmax(f, mm));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(kFull, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : kFltMax;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(kFull, v, o));
+    }
+    r = v;
+  }
+  if (threadIdx.x == 0) {
+    g->result = r;
+    g->cells_eval += ms->cells_eval;
+    g->cells_fp64 += ms->cells_fp64;
+    g->cells_vefd += ms->cells_vefd;
+    ms->cells_eval = ms->cells_fp64 = ms->cells_vefd = 0;
+    __threadfence();
+    finalize<KIND>(g, pd, active_pairs);
+    __threadfence();
   }
 }
 
@@ -872,6 +1005,9 @@ struct rfd_context {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // split pairs: the mirror kernel's stream, forked from and joined to `stream` by events
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int num_sms = 0;
   int grid[3] = {0, 0, 0};
   int team_grid[3] = {0, 0, 0};     // teams of the chosen shape (team_warps)
@@ -893,6 +1029,8 @@ struct rfd_context {
   // rows of the VE-FD and decision strips' boundary ring (RFD_TEAM_RING_ROWS, at least 2):
   // 0 keeps one row per strip unless a lone pair's rows do not fit (launch windows, run_batch)
   int team_ring_rows = 0;
+  // meet in the middle for lone pairs of at least this many team strips (RFD_SPLIT; 0: off)
+  int split_min = 64;
   void* dws = nullptr;
   size_t dws_size = 0;
   void* hws = nullptr;
@@ -914,13 +1052,15 @@ namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// The team kernel of the context's shape (warps per team) on its grid.
-template <int KIND>
-void launch_team(const rfd_context* ctx, const WaveArgs& wa, cudaStream_t st) {
+// The team kernel of the context's shape (warps per team) on its grid (grid > 0: that many
+// teams); MIR: the mirror kernel of split pairs.
+template <int KIND, bool MIR = false>
+void launch_team(const rfd_context* ctx, const WaveArgs& wa, cudaStream_t st, int grid = 0) {
+  const int g = grid > 0 ? grid : ctx->team_grid[KIND];
   if (ctx->team_warps == 4)
-    team_kernel<KIND, 4><<<ctx->team_grid[KIND], 128, team_smem_bytes<KIND>(), st>>>(wa);
+    team_kernel<KIND, 4, MIR><<<g, 128, team_smem_bytes<KIND>(), st>>>(wa);
   else
-    team_kernel<KIND, 8><<<ctx->team_grid[KIND], 256, team_smem_bytes<KIND>(), st>>>(wa);
+    team_kernel<KIND, 8, MIR><<<g, 256, team_smem_bytes<KIND>(), st>>>(wa);
 }
 
 // Row of rfd_context::team_grids for a team shape.
@@ -1277,7 +1417,25 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   const int64_t nmem = (int64_t)kpairs.size() * (karity > 1 ? karity - 1 : 0);
-  const int64_t nst = npairs + nmem;  // descriptors and states: the pairs', then the members'
+  // Meet in the middle for a lone pair (split_meet_kernel): the chain of its team strips,
+  // which bounds a long pair's VE-FD and decisions, runs as two halves at once.  Pairs of at
+  // least RFD_SPLIT strips (default 64; 0: never); not with k-ary members, launch windows,
+  // the solo strips or a lone decision (rfd_decide reports the right UB, which the meet does
+  // not form).  Results are bit-identical.  The pair's boundary rows k .. S - 1, which its
+  // forward half does not use, hold the mirror's rows (S rows in all, one more than unsplit);
+  // the probe rounds run as launches.
+  int64_t ksplit = 0;
+  if (npairs == 1 && mode != MODE_DECIDE && !ctx->solo && !twin && nmem == 0 &&
+      ctx->split_min > 0 && n1s[0] >= 2 && n2s[0] >= 2) {
+    const int64_t St = (trows(0) - 1 + 31) / 32;
+    if (St >= std::max(2, ctx->split_min)) ksplit = St / 2;
+  }
+  if (ksplit) {
+    dyn_cap = 0;
+    ntitems = (trows(0) - 1 + 31) / 32;  // k forward strips and S - k mirror strips
+  }
+  // descriptors and states: the pairs', then the members', then a split pair's mirror
+  const int64_t nst = npairs + nmem + (ksplit ? 1 : 0);
   auto mpair = [&](int64_t v) { return kpairs[v / (karity - 1)]; };
   // the members' strips join the team item list, interleaved with their pair's
   for (int64_t v = 0; v < nmem; ++v) ntitems += (trows(mpair(v)) + 31) / 32;
@@ -1293,7 +1451,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
   // launch windows: a ticket counter per window of every VE-FD phase and probe round
   const int64_t wbase = L.nlaunch + max_probes + 1;
-  const int64_t wtickets = nwin * (2 + std::max(max_probes, 1));
+  // (a split pair: one per VE-FD phase and probe round, for the mirror kernel)
+  const int64_t wtickets = (nwin + (ksplit ? 1 : 0)) * (2 + std::max(max_probes, 1));
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * (wbase + wtickets));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + kTraceW * kTrace));
@@ -1303,7 +1462,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // at least 32 point rows (the strip height the autotuner may pick); the coarse pair's DFD
     const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
     // team strips hand rows over through one row per strip (S - 1 rows)
-    L.ring_t[p] = ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
+    L.ring_t[p] = ksplit ? (int)St : ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
     L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
     L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
                       ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
@@ -1441,6 +1600,21 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       Dt.cstride = (long long)align_up((size_t)n1, 32);
       Dt.tstride = (long long)align_up((size_t)((n1 + 31) / 32), 32);
     }
+    if (ksplit) {
+      // the mirror sweeps rows 32k .. R - 1 from the top; its rows, tags and progress words
+      // are the pair's from strip k on
+      const int64_t St = (trows(p) - 1 + 31) / 32;
+      Dt.split = (int)ksplit;
+      PairDesc& Dm = ((PairDesc*)(hbase + L.h_tdescs))[npairs + nmem];
+      Dm = Dt;
+      Dm.split = -1;
+      Dm.mrow = Dt.n1 - 2;
+      Dm.n1 = Dt.n1 - 32 * (int)ksplit;
+      Dm.bnd = Dt.bnd + ksplit * Dt.cstride;
+      Dm.tags = Dt.tags + ksplit * Dt.tstride;
+      Dm.prog = Dt.prog + ksplit;
+      Dm.ring = (int)(St - ksplit);
+    }
     if (ck) {
       // the coarse pair: anchors of both curves, handing rows over through the pair's own
       // boundary rows (fewer rows of fewer columns).  A one-point curve keeps the exact DFD,
@@ -1506,6 +1680,14 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   std::vector<int> wstart(nwin + 1, 0);  // launch windows: first team item of each
+  if (ksplit) {
+    PairState& m = hs[npairs + nmem];
+    memset(&m, 0, sizeof(m));
+    m.epoch = 1;
+    m.dead_from = INT_MAX;
+    m.U = (double)INFINITY;
+    m.phase = PH_DONE;
+  }
   {
     int64_t k = 0;
     for (int64_t sidx = 0; sidx < maxS; ++sidx)
@@ -1515,7 +1697,12 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       }
     int2* ht = (int2*)(hbase + L.h_titems);
     k = 0;
-    for (int64_t sidx = 0; sidx < maxSt; ++sidx) {
+    // a split pair: its forward strips 0 .. k-1, then its mirror's (the two kernels' lists)
+    const int64_t St0 = ksplit ? (trows(0) - 1 + 31) / 32 : 0;
+    for (int64_t sidx = 0; sidx < ksplit; ++sidx) ht[k++] = make_int2(0, (int)sidx);
+    for (int64_t sidx = 0; sidx < St0 - ksplit; ++sidx)
+      ht[k++] = make_int2((int)(npairs + nmem), (int)sidx);
+    for (int64_t sidx = 0; sidx < (ksplit ? 0 : maxSt); ++sidx) {
       if (twin && sidx % twin == 0) wstart[sidx / twin] = (int)k;  // strip-major: windows are ranges
       for (int64_t q = 0; q < npairs; ++q) {
         const int p = order[q];
@@ -1667,12 +1854,36 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // with launch windows a reset and a launch per window, in strip order (each window's
     // items are a range of the strip-major item list).
     unsigned* wtick = counters + wbase;
-    auto team_round = [&](auto kind, int ph) {
+    auto team_round = [&](auto kind, int ph) -> int {
       constexpr int KIND = decltype(kind)::value;
+      if (ksplit) {
+        // the forward half here (items 0 .. k-1), the mirror half on the side stream (the
+        // other items, a ticket of its own), each on half the teams; then the meet
+        const int mi = (int)(npairs + nmem);
+        split_sync_kernel<<<1, 32, 0, st>>>(dt, ds, 0, mi, ph);
+        fill(ph);
+        const int half = std::max(1, ctx->team_grid[KIND] / 2);
+        WaveArgs wf = wa, wm = wa;
+        wf.nitems = (int)ksplit;
+        wm.items = wa.items + ksplit;
+        wm.nitems = L.ntitems - (int)ksplit;
+        wm.ticket = wtick++;
+        RFD_CUDA(cudaEventRecordWithFlags(ctx->fork_ev, st, cudaEventRecordDefault));
+        RFD_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+        launch_team<KIND, true>(ctx, wm, ctx->side, half);
+        RFD_CUDA(cudaGetLastError());
+        RFD_CUDA(cudaEventRecordWithFlags(ctx->join_ev, ctx->side, cudaEventRecordDefault));
+        launch_team<KIND>(ctx, wf, st, half);
+        RFD_CUDA(cudaGetLastError());
+        RFD_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
+        split_meet_kernel<KIND><<<1, 1024, 0, st>>>(dt, ds, 0, mi, ph, wa.error, wa.active_pairs);
+        launches += 3;
+        return RFD_OK;
+      }
       if (!twin) {
         fill(ph);
         launch_team<KIND>(ctx, wa, st);
-        return;
+        return RFD_OK;
       }
       WaveArgs w = wa;
       const int2* items0 = (const int2*)(dbase + L.titems);
@@ -1685,6 +1896,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         launch_team<KIND>(ctx, w, st);
       }
       launches += (int)(2 * nwin - 1);  // the caller counts one team launch
+      return RFD_OK;
     };
     if (mode != MODE_DECIDE) {
       wa.phase = PH_DFD;
@@ -1744,7 +1956,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         if (ctx->solo) {
           wave_kernel<K_VEFD><<<ctx->grid[K_VEFD], kBlock, 0, st>>>(wa);
         } else {
-          team_round(std::integral_constant<int, K_VEFD>{}, ph);
+          const int rc = team_round(std::integral_constant<int, K_VEFD>{}, ph);
+          if (rc) return rc;
         }
         RFD_CUDA(cudaGetLastError());
       }
@@ -1819,7 +2032,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       if (ctx->solo) {
         wave_kernel<K_DEC><<<ctx->grid[K_DEC], kBlock, 0, st>>>(wa);
       } else {
-        team_round(std::integral_constant<int, K_DEC>{}, PH_SEARCH);
+        const int rc = team_round(std::integral_constant<int, K_DEC>{}, PH_SEARCH);
+        if (rc) return rc;
       }
       RFD_CUDA(cudaGetLastError());
       ++launches;
@@ -1843,7 +2057,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                          ctx->solo, ctx->dfd_rows, ctx->dfd_skew, ctx->lockstep,
                          ctx->search_switch, ctx->search_window, ctx->team_warps,
                          (int)(ctx->spin_cycles >> 32),
-                         (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate, (int)twin};
+                         (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate, (int)twin,
+                         (int)ksplit};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));
@@ -2086,7 +2301,15 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
         cudaFuncSetAttribute(team_kernel<K_VEFD, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm_ve) != cudaSuccess ||
         cudaFuncSetAttribute(team_kernel<K_DEC, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm_dec) != cudaSuccess) {
+                             (int)sm_dec) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_VEFD, 8, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ve) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_DEC, 8, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dec) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_VEFD, 4, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_ve) != cudaSuccess ||
+        cudaFuncSetAttribute(team_kernel<K_DEC, 4, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_dec) != cudaSuccess) {
       delete c;
       return fail(RFD_ERR_CUDA, "cudaFuncSetAttribute(team smem)");
     }
@@ -2148,13 +2371,22 @@ int32_t rfd_context_create(int32_t device, rfd_context** out) {
     c->prof = pe && pe[0] == '1';
     c->dfd_ring_rows = env_rows("RFD_DFD_RING_ROWS", kDfdRingRows);
     c->team_ring_rows = env_rows("RFD_TEAM_RING_ROWS", 0);
+    if (const char* e = getenv("RFD_SPLIT"))
+      if (*e) c->split_min = std::max(0, atoi(e));
   }
   // wait budget: about 20 s at the maximum SM clock, or RFD_SPIN_CYCLES
   c->spin_default = (long long)prop.clockRate * 1000LL * 20LL;
   c->spin_cycles = env_spin_cycles(c->spin_default);
-  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->join_ev) cudaEventDestroy(c->join_ev);
     delete c;
-    return fail(RFD_ERR_CUDA, "cudaStreamCreate");
+    return fail(RFD_ERR_CUDA, "cudaStreamCreate / cudaEventCreate");
   }
   c->stream = c->own_stream;
   *out = c;
@@ -2170,6 +2402,9 @@ int32_t rfd_context_destroy(rfd_context* ctx) {
     if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
   delete ctx;
   return RFD_OK;
 }

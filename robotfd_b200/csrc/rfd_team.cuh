@@ -123,7 +123,28 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
 
 // ------------------------------------------------------------------ helpers (warps 1..3)
 
-template <int KIND, int D, int H /* helper warps */>
+// Mirror sweep (MIR, meet in the middle): the grid seen from its far corner.  Mirror cell
+// (i, j) is cell (a, b) = (mrow - i, C - 1 - j) of the pair, and its tile holds the values of
+// that cell's two entry edges - the right edge of cell (a - 1, b) (point p_a against segment
+// q_b q_{b+1}) and the top edge of cell (a, b - 1) (point q_b against segment p_a p_{a+1}) -
+// computed by the same functions from the same operands as the forward sweep's tiles, so
+// they are the same doubles.  VE-FD weights are used as they are (the min-max recurrence runs
+// backwards unchanged); a free interval [lo, hi] becomes [-hi, -lo] (exact), so that the
+// forward propagation, run on the mirrored grid, computes the negated upper ends of the
+// co-reachable parts (points from which the far corner can be reached); an empty interval
+// becomes (-3, -4), dead below -1.5.
+__device__ __forceinline__ void mirror_interval(double& lo, double& hi) {
+  if (lo < 0.0) {
+    lo = -3.0;
+    hi = -4.0;
+  } else {
+    const double l = lo;
+    lo = -hi;
+    hi = -l;
+  }
+}
+
+template <int KIND, int D, int H /* helper warps */, bool MIR = false>
 __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairState* st, int s,
                              TeamShared* sh, double2* tiles, double* stage, unsigned& seqH,
                              unsigned& seqS, int hw) {
@@ -135,7 +156,7 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
   const bool filt = KIND == K_DEC && st->filter;  // FP32 classification first (rfd_filter.h)
   const bool mat = KIND == K_DEC && st->formula == 1;  // materialised path's intervals
   RowData<KIND, D> row;
-  if (rowv) row.load(pd, i);
+  if (rowv) row.load(pd, MIR ? pd.mrow - i : i);
   const long long t0 = clock64();
   unsigned long long count = 0, count64 = 0;
   for (;;) {
@@ -163,14 +184,16 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
     {
       const int base = (c << 5) - 31;
       const int t = (hw << 5) + lane;
+      // (mirror: staged row jj holds point q_{C - base - jj} and the records of segment
+      // C - 1 - base - jj, so column j = base + jj reads q_b at jj + 1 and q_{b+1} at jj)
       for (int e = t; e < kStageRow * D; e += 32 * H) {
         const int jj = e / D, k = e - jj * D;
-        const int qi = min(max(base + jj, 0), C);
+        const int qi = MIR ? min(max(C - (base + jj), 0), C) : min(max(base + jj, 0), C);
         buf[k * kStageRow + jj] = __ldg(pd.Q + (size_t)qi * D + k);
       }
       constexpr int W = RecW<D>::value;
       for (int e = t; e < kStageRow - 1; e += 32 * H) {
-        const int j = min(max(base + e, 0), C - 1);
+        const int j = MIR ? min(max(C - 1 - (base + e), 0), C - 1) : min(max(base + e, 0), C - 1);
         const double2 a = __ldg(pd.colrec + (size_t)j * W + (W - 1));
         buf[3 * kStageRow + e] = a.x;
         buf[4 * kStageRow + e] = a.y;
@@ -186,8 +209,8 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
       const int jj = u - lane + 31;
 #pragma unroll
       for (int k = 0; k < D; ++k) {
-        col.qa[k] = buf[k * kStageRow + jj];
-        col.qb[k] = buf[k * kStageRow + jj + 1];
+        col.qa[k] = buf[k * kStageRow + jj + (MIR ? 1 : 0)];
+        col.qb[k] = buf[k * kStageRow + jj + (MIR ? 0 : 1)];
       }
       col.A = buf[3 * kStageRow + jj];
       col.inv2A = buf[4 * kStageRow + jj];
@@ -200,26 +223,33 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
 #pragma unroll
       for (int k = 0; k < D; ++k) qd[k] = __dsub_rn(col.qb[k], col.qa[k]);
       const bool ok = rowv && j >= 0 && j < C;
+      // the right edge's point (p_{i+1}; mirror: p_a) and the top edge's (q_{j+1}; mirror: q_b)
+      const double* xr = MIR ? row.a : row.b;
+      const double* xt = MIR ? col.qa : col.qb;
       if (KIND == K_DEC) {
         double rLB, rUB, tLB, tUB;
         // with the filter, an edge certainly empty or certainly whole takes the exact value
         // the FP64 code would write; the others are computed in FP64
         int cr = 0, ct = 0;
         if (filt) {
-          cr = interval_class32<D>(row.b, col.qa, qd, col.A, r2);
-          ct = interval_class32<D>(col.qb, row.a, row.ab, row.A, r2);
+          cr = interval_class32<D>(xr, col.qa, qd, col.A, r2);
+          ct = interval_class32<D>(xt, row.a, row.ab, row.A, r2);
         }
         if (cr == 0) {
-          free_interval<D>(row.b, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB, mat);
+          free_interval<D>(xr, col.qa, qd, col.A, col.inv2A, r2, rLB, rUB, mat);
         } else {
           rLB = cr == 1 ? -1.0 : 0.0;
           rUB = cr == 1 ? -2.0 : 1.0;
         }
         if (ct == 0) {
-          free_interval<D>(col.qb, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB, mat);
+          free_interval<D>(xt, row.a, row.ab, row.A, row.inv2A, r2, tLB, tUB, mat);
         } else {
           tLB = ct == 1 ? -1.0 : 0.0;
           tUB = ct == 1 ? -2.0 : 1.0;
+        }
+        if (MIR) {
+          mirror_interval(rLB, rUB);
+          mirror_interval(tLB, tUB);
         }
         count64 += (ok && (cr == 0 || ct == 0)) ? 1 : 0;
         if (ok) {
@@ -227,8 +257,14 @@ __device__ void team_helpers(const WaveArgs& wa, const PairDesc& pd, const PairS
           T1[(u << 5) + lane] = make_double2(tLB, tUB);
         }
       } else {
-        const double wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
-        const double wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
+        double wr, wt;
+        if constexpr (MIR) {
+          wr = pt_seg_sq<D>(row.a, col.qa, qd, col.A);
+          wt = pt_seg_sq<D>(col.qa, row.a, row.ab, row.A);
+        } else {
+          wr = pt_seg_sq<D>(row.b, col.qa, qd, col.A);
+          wt = pt_seg_sq<D>(col.qb, row.a, row.ab, row.A);
+        }
         if (ok) T0[(u << 5) + lane] = make_double2(wt, wr);
       }
       count += ok ? 1 : 0;
@@ -280,7 +316,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-template <int KIND, int D>
+template <int KIND, int D, bool MIR = false>
 __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState* st, const int s,
                                TeamShared* sh, const double2* tiles, unsigned& seqP,
                                unsigned& seqC) {
@@ -292,7 +328,16 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
   const double U = st->U;
   const bool dense = st->dense != 0;
   const bool has_prod = s > 0;
-  const bool has_cons = s + 1 < S;
+  // mirror sweep (meet in the middle): decision values live in [-1, 0], dead below -1.5
+  // (see mirror_interval); its last strip also hands its row on, to the meet kernel
+  constexpr bool mir = MIR;
+  const double dthr = mir ? -1.5 : 0.0;
+  const double dv = KIND == K_DEC ? (mir ? -3.0 : -1.0) : kFltMax;
+  auto isd = [U, dthr](double v) { return KIND == K_DEC ? v < dthr : v > U; };
+  const bool has_cons = s + 1 < S || mir;
+  // the lane whose row the strip hands on: 31, or, for the mirror's last strip, which may
+  // hold fewer than 32 rows, the lane of the grid's last row
+  const int olane = MIR ? (s + 1 < S ? 31 : ((R - 1) & 31)) : 31;
   const bool tr = pd.tr != 0;
 
   // Strip s writes boundary row s % ring (and its tags).  ring >= S - 1 unless the strips run
@@ -331,12 +376,15 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     out_prog->last_live = 0;
   }
   double bot;
-  if (KIND == K_DEC) bot = i == 0 ? 0.0 : -1.0;
+  // the mirror decision starts at the far corner: through the top edge of the pair's last
+  // cell (transposed grid) here, through its right edge as strip 0's input below
+  const bool inj = KIND == K_DEC && mir && !tr && st->corner != 0;
+  if (KIND == K_DEC) bot = mir ? ((i == 0 && tr && st->corner) ? -1.0 : dv) : (i == 0 ? 0.0 : -1.0);
   else bot = i == 0 ? st->seed : kFltMax;
-  double carry = dead_value<KIND>();
+  double carry = dv;
   double* out_row = sh->out_row;
-  out_row[lane] = dead_value<KIND>();
-  out_row[32 + lane] = dead_value<KIND>();
+  out_row[lane] = dv;
+  out_row[32 + lane] = dv;
   __syncwarp();
   unsigned first_live_out = kNone;
   int next_flush = 0;
@@ -383,8 +431,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     if (valid) st_relaxed_f64(out_bnd + col, v);
     wlo = min(wlo, k);
     whi = max(whi, k);
-    const unsigned live = __ballot_sync(kFull, valid && !is_dead<KIND>(v, U));
-    out_row[((k & 1) << 5) + lane] = dead_value<KIND>();
+    const unsigned live = __ballot_sync(kFull, valid && !isd(v));
+    out_row[((k & 1) << 5) + lane] = dv;
     __syncwarp();
     if (lane == 0) {
       if (live) {
@@ -440,7 +488,7 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
     pre_c = -1;
     if (!has_prod || (k << 5) >= C) return;
     const int col = (k << 5) + lane;
-    pre = col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dead_value<KIND>());
+    pre = col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dv);
     pre_c = k;
   };
 
@@ -451,7 +499,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         flush(next_flush, (next_flush & 7) == 7);
         ++next_flush;
       }
-    double inreg = dead_value<KIND>();
+    double inreg = dv;
+    if (inj && c == 0 && lane == 0) inreg = -1.0;  // column 0 of the mirror's first input row
     bool in_live = false;
     bool fast = false;
     if (has_prod && (c << 5) < C) {
@@ -462,14 +511,14 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       const int col = (c << 5) + lane;
       const unsigned need = (unsigned)min((c + 1) << 5, C);
       auto load = [&]() {
-        return col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dead_value<KIND>());
+        return col < C ? ld_relaxed_u64(in_bnd + col) : __double_as_longlong(dv);
       };
       unsigned long long v = pre_c == c ? pre : load();
       unsigned long long w = 0ull;
       for (int it = 0;; ++it) {
         if (__all_sync(kFull, v != kBndEmpty)) {
           inreg = __longlong_as_double(v);
-          in_live = __any_sync(kFull, col < C && !is_dead<KIND>(inreg, U));
+          in_live = __any_sync(kFull, col < C && !isd(inreg));
           fast = true;
           break;
         }
@@ -493,7 +542,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
           if (col < C) inreg = __ldcg(in_bnd + col);
         }
       } else {
-        in_live = !is_dead<KIND>(inreg, U);
+        // (mirror: warp-uniform, only the decision's column 0 can be live here; otherwise
+        // every lane's input is dead)
+        if (MIR) in_live = __any_sync(kFull, !isd(inreg));
+        else in_live = !isd(inreg);
       }
     }
     if (in_live && !seen_live) {
@@ -516,8 +568,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
       if (lane == 0) trace[1] = global_ns();
     }
     if (!dense && !in_live) {
-      const bool ldead = (!rowv || is_dead<KIND>(bot, U) || ((c << 5) - lane >= C)) &&
-                         is_dead<KIND>(carry, U);
+      const bool ldead = (!rowv || isd(bot) || ((c << 5) - lane >= C)) &&
+                         isd(carry);
       if (__all_sync(kFull, ldead)) {
         int nc = -1;
         if (has_prod && (c << 5) < C) {
@@ -598,10 +650,10 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
           next_flush = nc - 1;
           publish_cols(min((nc - 1) << 5, C));
         }
-        carry = dead_value<KIND>();
+        carry = dv;
         __syncwarp();
-        out_row[lane] = dead_value<KIND>();
-        out_row[32 + lane] = dead_value<KIND>();
+        out_row[lane] = dv;
+        out_row[32 + lane] = dv;
         __syncwarp();
         c = nc;
         if (pending != c) {
@@ -651,17 +703,17 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         if (KIND == K_DEC) {
           // same propagation as the solo cell, written with selects (no divergence)
           const double rLB = ta.x, rUB = ta.y, tLB = tb.x, tUB = tb.y;
-          const bool bdead = bot < 0.0, ldead = left < 0.0;
+          const bool bdead = bot < dthr, ldead = left < dthr;
           const bool rinv = (left > rUB) || ldead;
           const bool tinv = (bot > tUB) || bdead;
           const double rm = dmax(rLB, left);
           const double tm = dmax(tLB, bot);
-          ncarry = bdead ? (rinv ? -1.0 : rm) : rLB;
+          ncarry = bdead ? (rinv ? dv : rm) : rLB;
           // the result is the last cell's right edge: on a transposed grid, its top edge
           nres = IN ? 0.0
                     : (tr ? (ldead ? (tinv ? -2.0 : tUB) : tUB)
                           : (bdead ? (rinv ? -2.0 : rUB) : rUB));
-          nbot = ldead ? (tinv ? -1.0 : tm) : tLB;
+          nbot = ldead ? (tinv ? dv : tm) : tLB;
         } else {
           const double in = dmin(left, bot);
           const double top = dmax(ta.x, in);
@@ -673,8 +725,8 @@ __device__ int team_propagator(const WaveArgs& wa, const PairDesc& pd, PairState
         carry = act ? ncarry : carry;
         bot = act ? nbot : bot;
         if (!IN && act && last_row && j == C - 1) res = nres;
-        // lane 31 produced column (c << 5) + u - 31 of the strip's last row
-        if (lane == 31) out_row[((c << 5) + u - 31) & 63] = carry;
+        // lane olane (31) produced column (c << 5) + u - olane of the strip's last row
+        if (lane == olane) out_row[((c << 5) + u - olane) & 63] = carry;
       }
     };
     if (c >= 1 && (c << 5) + 33 <= C && (s + 1) * 32 <= R) steps(std::true_type{});
