@@ -169,7 +169,9 @@ int32_t rfd_context_destroy(rfd_context* ctx);
    contexts and the budget of rfd_decide_noalloc.  (The reference's spin-waits are unbounded,
    src/intersection_algorithm_in_parallel.cu:304-306, :332-334.) */
 int32_t rfd_context_set_wait_budget(rfd_context* ctx, int64_t cycles);
-/* Use a caller stream (cudaStream_t) instead of the context's own; NULL restores it. */
+/* Use a caller stream (cudaStream_t) instead of the context's own; NULL restores it.  A lone
+   pair split in two halves (RFD_SPLIT) runs one half on a second stream the context owns,
+   forked from and joined back to this stream with events, so the call stays ordered on it. */
 int32_t rfd_context_set_stream(rfd_context* ctx, void* stream);
 /* Phase timing with CUDA events on the context's stream (off by default; no reference
    counterpart - the reference prints host wall times, src/frechet.cpp:65-71).
