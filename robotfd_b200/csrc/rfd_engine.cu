@@ -797,11 +797,10 @@ __device__ void split_corner(const PairDesc& pd, PairState* m, const PairState* 
   }
 }
 
-// Before each team launch of a split pair (descriptor p, mirror m): the mirror follows the
-// pair's running phase - radius, pruning bound, epoch, options - with fresh counters and its
-// far corner set up; idle when the pair does not run the phase.  One thread.
-__global__ void split_sync_kernel(const PairDesc* pairs, PairState* sts, int p, int m, int phase) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Mirror m of pair p before a team launch: it follows the pair's running phase - radius,
+// pruning bound, epoch, options - with fresh counters and its far corner set up; idle when
+// the pair does not run the phase.
+__device__ void split_sync_one(const PairDesc* pairs, PairState* sts, int p, int m, int phase) {
   const PairState* g = sts + p;
   PairState* ms = sts + m;
   const bool run = g->phase == phase && g->active;
@@ -824,13 +823,24 @@ __global__ void split_sync_kernel(const PairDesc* pairs, PairState* sts, int p, 
   __threadfence();
 }
 
-// After each team launch of a split pair: the meet (see above) gives the phase's result,
-// which then ends the phase as the unsplit sweep's last strip would (finalize).  Unwritten
-// boundary words are NaN (all ones) and fail every comparison, i.e. count as dead.  One CTA.
+// Before each team launch with split pairs: every mirror (descriptors mbase .. mbase + nm - 1,
+// each naming its pair p by split = -(p + 1)) set up by split_sync_one.  One thread a mirror.
+__global__ void split_sync_kernel(const PairDesc* pairs, PairState* sts, int mbase, int nm,
+                                  int phase) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nm; v += gridDim.x * blockDim.x)
+    split_sync_one(pairs, sts, -pairs[mbase + v].split - 1, mbase + v, phase);
+}
+
+// After each team launch with split pairs: for each (one CTA a mirror, mbase + blockIdx.x) the
+// meet (see above) gives its pair's result for the phase, which then ends the phase as the
+// unsplit sweep's last strip would (finalize).  Unwritten boundary words are NaN (all ones)
+// and fail every comparison, i.e. count as dead.
 template <int KIND>
 __global__ void __launch_bounds__(1024) split_meet_kernel(const PairDesc* pairs, PairState* sts,
-                                                          int p, int m, int phase, const int* error,
+                                                          int mbase, int phase, const int* error,
                                                           int* active_pairs) {
+  const int m = mbase + blockIdx.x;
+  const int p = -pairs[m].split - 1;
   PairState* g = sts + p;
   PairState* ms = sts + m;
   if (ld_volatile(&g->phase) != phase || !ld_volatile(&g->active) || ld_volatile(error)) return;
@@ -1417,25 +1427,36 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   const int64_t nmem = (int64_t)kpairs.size() * (karity > 1 ? karity - 1 : 0);
-  // Meet in the middle for a lone pair (split_meet_kernel): the chain of its team strips,
-  // which bounds a long pair's VE-FD and decisions, runs as two halves at once.  Pairs of at
-  // least RFD_SPLIT strips (default 64; 0: never); not with k-ary members, launch windows,
-  // the solo strips or a lone decision (rfd_decide reports the right UB, which the meet does
-  // not form).  Results are bit-identical.  The pair's boundary rows k .. S - 1, which its
-  // forward half does not use, hold the mirror's rows (S rows in all, one more than unsplit);
-  // the probe rounds run as launches.
-  int64_t ksplit = 0;
-  if (npairs == 1 && mode != MODE_DECIDE && !ctx->solo && !twin && nmem == 0 &&
-      ctx->split_min > 0 && n1s[0] >= 2 && n2s[0] >= 2) {
-    const int64_t St = (trows(0) - 1 + 31) / 32;
-    if (St >= std::max(2, ctx->split_min)) ksplit = St / 2;
-  }
-  if (ksplit) {
+  // Meet in the middle (split_meet_kernel): in a call of at most kSplitPairs pairs, the chain
+  // of a pair's team strips, which bounds a long pair's VE-FD and decisions, runs as two halves
+  // at once.  Pairs of at least RFD_SPLIT strips (default 64; 0: never); not with k-ary
+  // members, launch windows, the solo strips or rfd_decide (which reports the right UB, which
+  // the meet does not form).  Results are bit-identical.  A split pair's boundary rows
+  // k .. S - 1, which its forward half does not use, hold its mirror's rows (S rows in all,
+  // one more than unsplit); the probe rounds run as launches.  Larger calls keep every team
+  // busy with pairs already and keep the continuous search.
+  constexpr int64_t kSplitPairs = 8;
+  std::vector<int64_t> ksp(npairs, 0);  // forward strips of a split pair (0: not split)
+  std::vector<int64_t> mirror_of(npairs, -1);  // its mirror's descriptor index
+  int64_t nsplit = 0, nfwd = 0, nmir = 0;  // split pairs; forward and mirror team items
+  if (npairs <= kSplitPairs && mode != MODE_DECIDE && !ctx->solo && !twin && nmem == 0 &&
+      ctx->split_min > 0)
+    for (int64_t p = 0; p < npairs; ++p) {
+      const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
+      if (n1s[p] >= 2 && n2s[p] >= 2 && St >= std::max(2, ctx->split_min)) {
+        ksp[p] = St / 2;
+        mirror_of[p] = npairs + nmem + nsplit++;
+        nmir += St - ksp[p];
+      }
+    }
+  if (nsplit) {
     dyn_cap = 0;
-    ntitems = (trows(0) - 1 + 31) / 32;  // k forward strips and S - k mirror strips
+    for (int64_t p = 0; p < npairs; ++p) nfwd += ksp[p] ? ksp[p] : (trows(p) + 31) / 32;
+    ntitems = nfwd + nmir;  // the forward kernel's list, then the mirror kernel's
   }
-  // descriptors and states: the pairs', then the members', then a split pair's mirror
-  const int64_t nst = npairs + nmem + (ksplit ? 1 : 0);
+  const int64_t mbase = npairs + nmem;  // the first mirror descriptor
+  // descriptors and states: the pairs', then the members', then the split pairs' mirrors
+  const int64_t nst = npairs + nmem + nsplit;
   auto mpair = [&](int64_t v) { return kpairs[v / (karity - 1)]; };
   // the members' strips join the team item list, interleaved with their pair's
   for (int64_t v = 0; v < nmem; ++v) ntitems += (trows(mpair(v)) + 31) / 32;
@@ -1452,7 +1473,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   // launch windows: a ticket counter per window of every VE-FD phase and probe round
   const int64_t wbase = L.nlaunch + max_probes + 1;
   // (a split pair: one per VE-FD phase and probe round, for the mirror kernel)
-  const int64_t wtickets = (nwin + (ksplit ? 1 : 0)) * (2 + std::max(max_probes, 1));
+  const int64_t wtickets = (nwin + (nsplit ? 1 : 0)) * (2 + std::max(max_probes, 1));
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * (wbase + wtickets));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + kTraceW * kTrace));
@@ -1462,7 +1483,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // at least 32 point rows (the strip height the autotuner may pick); the coarse pair's DFD
     const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
     // team strips hand rows over through one row per strip (S - 1 rows)
-    L.ring_t[p] = ksplit ? (int)St : ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
+    L.ring_t[p] = ksp[p] ? (int)St : ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
     L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
     L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
                       ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
@@ -1600,14 +1621,14 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       Dt.cstride = (long long)align_up((size_t)n1, 32);
       Dt.tstride = (long long)align_up((size_t)((n1 + 31) / 32), 32);
     }
-    if (ksplit) {
+    if (ksp[p]) {
       // the mirror sweeps rows 32k .. R - 1 from the top; its rows, tags and progress words
-      // are the pair's from strip k on
-      const int64_t St = (trows(p) - 1 + 31) / 32;
+      // are the pair's from strip k on; split = -(p + 1) names its pair
+      const int64_t St = (trows(p) - 1 + 31) / 32, ksplit = ksp[p];
       Dt.split = (int)ksplit;
-      PairDesc& Dm = ((PairDesc*)(hbase + L.h_tdescs))[npairs + nmem];
+      PairDesc& Dm = ((PairDesc*)(hbase + L.h_tdescs))[mirror_of[p]];
       Dm = Dt;
-      Dm.split = -1;
+      Dm.split = -(int)(p + 1);
       Dm.mrow = Dt.n1 - 2;
       Dm.n1 = Dt.n1 - 32 * (int)ksplit;
       Dm.bnd = Dt.bnd + ksplit * Dt.cstride;
@@ -1680,8 +1701,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
   }
   std::vector<int> wstart(nwin + 1, 0);  // launch windows: first team item of each
-  if (ksplit) {
-    PairState& m = hs[npairs + nmem];
+  for (int64_t v = mbase; v < nst; ++v) {  // mirrors: idle until split_sync_kernel
+    PairState& m = hs[v];
     memset(&m, 0, sizeof(m));
     m.epoch = 1;
     m.dead_from = INT_MAX;
@@ -1697,12 +1718,22 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       }
     int2* ht = (int2*)(hbase + L.h_titems);
     k = 0;
-    // a split pair: its forward strips 0 .. k-1, then its mirror's (the two kernels' lists)
-    const int64_t St0 = ksplit ? (trows(0) - 1 + 31) / 32 : 0;
-    for (int64_t sidx = 0; sidx < ksplit; ++sidx) ht[k++] = make_int2(0, (int)sidx);
-    for (int64_t sidx = 0; sidx < St0 - ksplit; ++sidx)
-      ht[k++] = make_int2((int)(npairs + nmem), (int)sidx);
-    for (int64_t sidx = 0; sidx < (ksplit ? 0 : maxSt); ++sidx) {
+    // with split pairs: the forward kernel's list (every pair, a split pair's strips 0 .. k-1),
+    // then the mirror kernel's, each strip-major
+    if (nsplit) {
+      for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+        for (int64_t q = 0; q < npairs; ++q) {
+          const int p = order[q];
+          if (sidx < (ksp[p] ? ksp[p] : (trows(p) + 31) / 32)) ht[k++] = make_int2(p, (int)sidx);
+        }
+      for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+        for (int64_t q = 0; q < npairs; ++q) {
+          const int p = order[q];
+          if (ksp[p] && sidx < (trows(p) - 1 + 31) / 32 - ksp[p])
+            ht[k++] = make_int2((int)mirror_of[p], (int)sidx);
+        }
+    }
+    for (int64_t sidx = 0; sidx < (nsplit ? 0 : maxSt); ++sidx) {
       if (twin && sidx % twin == 0) wstart[sidx / twin] = (int)k;  // strip-major: windows are ranges
       for (int64_t q = 0; q < npairs; ++q) {
         const int p = order[q];
@@ -1856,17 +1887,16 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     unsigned* wtick = counters + wbase;
     auto team_round = [&](auto kind, int ph) -> int {
       constexpr int KIND = decltype(kind)::value;
-      if (ksplit) {
-        // the forward half here (items 0 .. k-1), the mirror half on the side stream (the
-        // other items, a ticket of its own), each on half the teams; then the meet
-        const int mi = (int)(npairs + nmem);
-        split_sync_kernel<<<1, 32, 0, st>>>(dt, ds, 0, mi, ph);
+      if (nsplit) {
+        // the forward halves here (the first nfwd items), the mirror halves on the side stream
+        // (the others, a ticket of their own), each on half the teams; then the meets
+        split_sync_kernel<<<1, 32, 0, st>>>(dt, ds, (int)mbase, (int)nsplit, ph);
         fill(ph);
         const int half = std::max(1, ctx->team_grid[KIND] / 2);
         WaveArgs wf = wa, wm = wa;
-        wf.nitems = (int)ksplit;
-        wm.items = wa.items + ksplit;
-        wm.nitems = L.ntitems - (int)ksplit;
+        wf.nitems = (int)nfwd;
+        wm.items = wa.items + nfwd;
+        wm.nitems = (int)nmir;
         wm.ticket = wtick++;
         RFD_CUDA(cudaEventRecordWithFlags(ctx->fork_ev, st, cudaEventRecordDefault));
         RFD_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
@@ -1876,7 +1906,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         launch_team<KIND>(ctx, wf, st, half);
         RFD_CUDA(cudaGetLastError());
         RFD_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
-        split_meet_kernel<KIND><<<1, 1024, 0, st>>>(dt, ds, 0, mi, ph, wa.error, wa.active_pairs);
+        split_meet_kernel<KIND><<<(int)nsplit, 1024, 0, st>>>(dt, ds, (int)mbase, ph, wa.error,
+                                                              wa.active_pairs);
         launches += 3;
         return RFD_OK;
       }
@@ -2058,7 +2089,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
                          ctx->search_switch, ctx->search_window, ctx->team_warps,
                          (int)(ctx->spin_cycles >> 32),
                          (int)(ctx->spin_cycles & 0xffffffff), karity, kary_gate, (int)twin,
-                         (int)ksplit};
+                         (int)nsplit, ctx->split_min};
     const void* ptrs[] = {dbase, hbase, gmodel, gmodel ? rfd_mlp::buffers_id(gmodel) : nullptr,
                           (const void*)st};
     mix(flags, sizeof(flags));

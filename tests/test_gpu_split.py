@@ -121,3 +121,31 @@ def test_split_batch_of_one_and_graph(split_ctx, plain_ctx, built):
         got = split_ctx.distance_batch([P], [Q], precise=True, graph=graph)[0]
         for k in EXACT:
             assert got[k] == want[k], (graph, k, got[k], want[k])
+
+
+def test_split_small_batch(split_ctx, plain_ctx, built):
+    """A call of a few pairs (at most 8 split): each pair of enough strips gets its own mirror
+    and meet, smaller pairs run whole in the same launches; plain, learned and coarse-bound
+    forms field for field against the unsplit context, the plain form against the oracle."""
+    specs = [(1, 3, 3000, 2800), (0, 2, 900, 2500), (1, 2, 2100, 90), (0, 3, 40, 50),
+             (1, 3, 1500, 1700)]
+    pairs = [built.gen_pair(st, d, n1, n2, 100.0 if st else 1.0, 0.1, 59, k)
+             for k, (st, d, n1, n2) in enumerate(specs)]
+    Ps, Qs = [a for a, _ in pairs], [b for _, b in pairs]
+    model = built.Model.pretrained(0)
+    try:
+        for kw in (dict(precise=True), dict(precise=True, model=model, coarse_ub=6),
+                   dict(precise=False)):
+            a = plain_ctx.distance_batch(Ps, Qs, **kw)
+            b = split_ctx.distance_batch(Ps, Qs, **kw)
+            for n, (x, y) in enumerate(zip(a, b)):
+                for k in EXACT:
+                    assert x[k] == y[k], (kw, n, k, x[k], y[k])
+    finally:
+        model.close()
+    got = split_ctx.distance_batch(Ps, Qs, precise=True)
+    th = oracle.max_threads()
+    for n in (0, 1, 3):
+        want = oracle.distance(Ps[n], Qs[n], stop_mode=1, quirks=False, threads=th)
+        for k in ("distance", "dfd", "vefd", "probes"):
+            assert got[n][k] == want[k], (n, k, got[n][k], want[k])
