@@ -419,7 +419,9 @@ __global__ void team_window_fill_kernel(const PairDesc* pairs, const PairState* 
     if (st[p].phase != phase || !st[p].active) continue;
     const PairDesc pd = pairs[p];
     const int S = (pd.n1 - 1 + 31) / 32;
-    const int s1 = min(s0 + count, S - 1);  // strips with a consumer write a row
+    // strips with a consumer write a row: all S - 1 of them, a split pair's forward half all
+    // its `split` strips, a mirror (split < 0) all S
+    const int s1 = min(s0 + count, pd.split > 0 ? pd.split : (pd.split < 0 ? S : S - 1));
     for (int s = s0 + (int)blockIdx.x; s < s1; s += gridDim.x) {
       const long long r = s % pd.ring;
       // cstride is a multiple of 32 doubles and bnd 256-byte aligned: 16-byte stores
@@ -1379,7 +1381,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     }
     if (twin >= maxSt) twin = 0;  // one window holds every strip: nothing to gain
   }
-  const int64_t nwin = twin ? (maxSt + twin - 1) / twin : 0;
+  int64_t nwin = twin ? (maxSt + twin - 1) / twin : 0;  // (recomputed for split pairs below)
   // Continuous search: a queue slot for every strip of every probe
   // (at most 512 MB; past that, and for the solo strips, one launch per probe round)
   int64_t dyn_cap = 0;
@@ -1439,7 +1441,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   std::vector<int64_t> ksp(npairs, 0);  // forward strips of a split pair (0: not split)
   std::vector<int64_t> mirror_of(npairs, -1);  // its mirror's descriptor index
   int64_t nsplit = 0, nfwd = 0, nmir = 0;  // split pairs; forward and mirror team items
-  if (npairs <= kSplitPairs && mode != MODE_DECIDE && !ctx->solo && !twin && nmem == 0 &&
+  if (npairs <= kSplitPairs && mode != MODE_DECIDE && !ctx->solo && nmem == 0 &&
       ctx->split_min > 0)
     for (int64_t p = 0; p < npairs; ++p) {
       const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
@@ -1453,6 +1455,18 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     dyn_cap = 0;
     for (int64_t p = 0; p < npairs; ++p) nfwd += ksp[p] ? ksp[p] : (trows(p) + 31) / 32;
     ntitems = nfwd + nmir;  // the forward kernel's list, then the mirror kernel's
+  }
+  if (nsplit && twin) {
+    // launch windows of both halves: window g runs strips g W .. g W + W - 1 of every
+    // forward half and of every mirror, each half through a ring of its own (W + 1 rows, or
+    // its strips if fewer); with windows chosen by the budget, W is halved for the two rings
+    if (ctx->team_ring_rows < 2) twin = std::max<int64_t>(1, (twin + 1) / 2 - 1);
+    int64_t most = 0;
+    for (int64_t p = 0; p < npairs; ++p) {
+      const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
+      most = std::max(most, ksp[p] ? std::max(ksp[p], St - ksp[p]) : (trows(p) + 31) / 32);
+    }
+    nwin = (most + twin - 1) / twin;
   }
   const int64_t mbase = npairs + nmem;  // the first mirror descriptor
   // descriptors and states: the pairs', then the members', then the split pairs' mirrors
@@ -1472,8 +1486,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
   L.nlaunch = 3 + max_probes + (mode == MODE_DECIDE ? 1 : 0) + 2;
   // launch windows: a ticket counter per window of every VE-FD phase and probe round
   const int64_t wbase = L.nlaunch + max_probes + 1;
-  // (a split pair: one per VE-FD phase and probe round, for the mirror kernel)
-  const int64_t wtickets = (nwin + (nsplit ? 1 : 0)) * (2 + std::max(max_probes, 1));
+  // (split pairs: one per VE-FD phase and probe round for the mirror kernel, or, with
+  // windows, one per window for each half)
+  const int64_t wtickets =
+      (nsplit ? (twin ? 2 * nwin : 1) : nwin) * (2 + std::max(max_probes, 1));
   L.zero_begin = off;
   L.counters = take(sizeof(unsigned) * (wbase + wtickets));
   const size_t prof_off = take(sizeof(unsigned long long) * (kTraceBase + kTraceW * kTrace));
@@ -1483,7 +1499,10 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // at least 32 point rows (the strip height the autotuner may pick); the coarse pair's DFD
     const int64_t St = (std::max<int64_t>(trows(p) - 1, 0) + 31) / 32;
     // team strips hand rows over through one row per strip (S - 1 rows)
-    L.ring_t[p] = ksp[p] ? (int)St : ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
+    // (a split pair: its forward ring, then its mirror's - S rows, or two window rings)
+    L.ring_t[p] = ksp[p] ? (int)(twin ? std::min(twin + 1, ksp[p]) + std::min(twin + 1, St - ksp[p])
+                                      : St)
+                         : ring_of(St, twin ? (int)(twin + 1) : INT32_MAX);
     L.ring_d[p] = ring_of((n1s[p] + 31) / 32, ctx->dfd_ring_rows);
     L.ring_c[p] = ck && n1s[p] >= 2 && n2s[p] >= 2
                       ? ring_of((coarse_n(n1s[p]) + 31) / 32, ctx->dfd_ring_rows) : 1;
@@ -1625,16 +1644,20 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       // the mirror sweeps rows 32k .. R - 1 from the top; its rows, tags and progress words
       // are the pair's from strip k on; split = -(p + 1) names its pair
       const int64_t St = (trows(p) - 1 + 31) / 32, ksplit = ksp[p];
+      // the halves' rings: every strip's row, or, in launch windows, W + 1 rows each
+      const int64_t rf = twin ? std::min(twin + 1, ksplit) : ksplit;
+      const int64_t rm = twin ? std::min(twin + 1, St - ksplit) : St - ksplit;
       Dt.split = (int)ksplit;
+      Dt.ring = (int)rf;
       PairDesc& Dm = ((PairDesc*)(hbase + L.h_tdescs))[mirror_of[p]];
       Dm = Dt;
       Dm.split = -(int)(p + 1);
       Dm.mrow = Dt.n1 - 2;
       Dm.n1 = Dt.n1 - 32 * (int)ksplit;
-      Dm.bnd = Dt.bnd + ksplit * Dt.cstride;
-      Dm.tags = Dt.tags + ksplit * Dt.tstride;
+      Dm.bnd = Dt.bnd + rf * Dt.cstride;
+      Dm.tags = Dt.tags + rf * Dt.tstride;
       Dm.prog = Dt.prog + ksplit;
-      Dm.ring = (int)(St - ksplit);
+      Dm.ring = (int)rm;
     }
     if (ck) {
       // the coarse pair: anchors of both curves, handing rows over through the pair's own
@@ -1700,7 +1723,8 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
       hs[p].kary_cap = karity - 1;
     }
   }
-  std::vector<int> wstart(nwin + 1, 0);  // launch windows: first team item of each
+  // launch windows: first team item of each (split pairs: forward windows, then the mirrors')
+  std::vector<int> wstart(2 * (nwin + 1), 0);
   for (int64_t v = mbase; v < nst; ++v) {  // mirrors: idle until split_sync_kernel
     PairState& m = hs[v];
     memset(&m, 0, sizeof(m));
@@ -1721,17 +1745,24 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
     // with split pairs: the forward kernel's list (every pair, a split pair's strips 0 .. k-1),
     // then the mirror kernel's, each strip-major
     if (nsplit) {
-      for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+      const int64_t lim = twin ? nwin * twin : maxSt;  // (windows cover every strip)
+      for (int64_t sidx = 0; sidx < lim; ++sidx) {
+        if (twin && sidx % twin == 0) wstart[sidx / twin] = (int)k;
         for (int64_t q = 0; q < npairs; ++q) {
           const int p = order[q];
           if (sidx < (ksp[p] ? ksp[p] : (trows(p) + 31) / 32)) ht[k++] = make_int2(p, (int)sidx);
         }
-      for (int64_t sidx = 0; sidx < maxSt; ++sidx)
+      }
+      if (twin) wstart[nwin] = (int)k;
+      for (int64_t sidx = 0; sidx < lim; ++sidx) {
+        if (twin && sidx % twin == 0) wstart[nwin + 1 + sidx / twin] = (int)k;
         for (int64_t q = 0; q < npairs; ++q) {
           const int p = order[q];
           if (ksp[p] && sidx < (trows(p) - 1 + 31) / 32 - ksp[p])
             ht[k++] = make_int2((int)mirror_of[p], (int)sidx);
         }
+      }
+      if (twin) wstart[2 * nwin + 1] = (int)k;
     }
     for (int64_t sidx = 0; sidx < (nsplit ? 0 : maxSt); ++sidx) {
       if (twin && sidx % twin == 0) wstart[sidx / twin] = (int)k;  // strip-major: windows are ranges
@@ -1744,7 +1775,7 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         }
       }
     }
-    if (twin) wstart[nwin] = (int)k;
+    if (twin && !nsplit) wstart[nwin] = (int)k;
   }
 
   if (!on_device) {
@@ -1891,21 +1922,46 @@ int run_batch(rfd_context* ctx, int64_t npairs, const double* const* c1s, const 
         // the forward halves here (the first nfwd items), the mirror halves on the side stream
         // (the others, a ticket of their own), each on half the teams; then the meets
         split_sync_kernel<<<1, 32, 0, st>>>(dt, ds, (int)mbase, (int)nsplit, ph);
-        fill(ph);
         const int half = std::max(1, ctx->team_grid[KIND] / 2);
-        WaveArgs wf = wa, wm = wa;
-        wf.nitems = (int)nfwd;
-        wm.items = wa.items + nfwd;
-        wm.nitems = (int)nmir;
-        wm.ticket = wtick++;
-        RFD_CUDA(cudaEventRecordWithFlags(ctx->fork_ev, st, cudaEventRecordDefault));
-        RFD_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
-        launch_team<KIND, true>(ctx, wm, ctx->side, half);
-        RFD_CUDA(cudaGetLastError());
-        RFD_CUDA(cudaEventRecordWithFlags(ctx->join_ev, ctx->side, cudaEventRecordDefault));
-        launch_team<KIND>(ctx, wf, st, half);
-        RFD_CUDA(cudaGetLastError());
-        RFD_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
+        // one pass: the forward list here, the mirror list on the side stream, together
+        auto both = [&](const WaveArgs& wf, const WaveArgs& wm) -> int {
+          RFD_CUDA(cudaEventRecordWithFlags(ctx->fork_ev, st, cudaEventRecordDefault));
+          RFD_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+          if (wm.nitems > 0) launch_team<KIND, true>(ctx, wm, ctx->side, half);
+          RFD_CUDA(cudaGetLastError());
+          RFD_CUDA(cudaEventRecordWithFlags(ctx->join_ev, ctx->side, cudaEventRecordDefault));
+          if (wf.nitems > 0) launch_team<KIND>(ctx, wf, st, half);
+          RFD_CUDA(cudaGetLastError());
+          RFD_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
+          return RFD_OK;
+        };
+        if (!twin) {
+          fill(ph);
+          WaveArgs wf = wa, wm = wa;
+          wf.nitems = (int)nfwd;
+          wm.items = wa.items + nfwd;
+          wm.nitems = (int)nmir;
+          wm.ticket = wtick++;
+          const int rc = both(wf, wm);
+          if (rc) return rc;
+        } else {
+          // launch windows: window g of every half at once, its rows reset first
+          const int2* items0 = (const int2*)(dbase + L.titems);
+          for (int64_t g = 0; g < nwin; ++g) {
+            team_window_fill_kernel<<<dim3(fill_gx, fill_gy), 256, 0, st>>>(
+                dt, ds, (int)nst, ph, (int)(g * twin), (int)twin);
+            WaveArgs wf = wa, wm = wa;
+            wf.items = items0 + wstart[g];
+            wf.nitems = wstart[g + 1] - wstart[g];
+            wf.ticket = wtick++;
+            wm.items = items0 + wstart[nwin + 1 + g];
+            wm.nitems = wstart[nwin + 2 + g] - wstart[nwin + 1 + g];
+            wm.ticket = wtick++;
+            const int rc = both(wf, wm);
+            if (rc) return rc;
+          }
+          launches += (int)(3 * nwin - 2);
+        }
         split_meet_kernel<KIND><<<(int)nsplit, 1024, 0, st>>>(dt, ds, (int)mbase, ph, wa.error,
                                                               wa.active_pairs);
         launches += 3;

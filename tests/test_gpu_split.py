@@ -149,3 +149,28 @@ def test_split_small_batch(split_ctx, plain_ctx, built):
         want = oracle.distance(Ps[n], Qs[n], stop_mode=1, quirks=False, threads=th)
         for k in ("distance", "dfd", "vefd", "probes"):
             assert got[n][k] == want[k], (n, k, got[n][k], want[k])
+
+
+@pytest.fixture(scope="module", params=[2, 3, 7])
+def win_split_ctx(built, request):
+    c = _ctx(built, RFD_SPLIT=2, RFD_TEAM_RING_ROWS=request.param)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("style,d,n1,n2", PAIRS[:5])
+def test_split_in_launch_windows(win_split_ctx, built, style, d, n1, n2):
+    """Both halves in launch windows (rings of 2, 3 and 7 rows each: window g of every half
+    at once, the meet after the last): solves, bounds and the reference mode against the
+    oracle."""
+    P, Q = built.gen_pair(style, d, n1, n2, 100.0 if style else 1.0, 0.1, 61, n1)
+    th = oracle.max_threads()
+    want = oracle.distance(P, Q, stop_mode=1, quirks=False, threads=th)
+    got = win_split_ctx.distance(P, Q, precise=True)
+    for k in ("distance", "dfd", "vefd", "lb", "ub", "probes"):
+        assert got[k] == want[k], (k, got[k], want[k])
+    assert win_split_ctx.bounds(P, Q, quirks=False, dense=True) == (want["dfd"], want["vefd"])
+    want = oracle.distance(P, Q, stop_mode=0, quirks=True, threads=th)
+    got = win_split_ctx.distance(P, Q)
+    for k in ("distance", "lb", "ub", "probes"):
+        assert got[k] == want[k], (k, got[k], want[k])
