@@ -1,9 +1,9 @@
-// "Team" strips: one CTA of 4 warps per 32-row strip for the VE-FD and decision DPs.
+// "Team" strips: one CTA of 8 (or 4) warps per 32-row strip for the VE-FD and decision DPs.
 //
 // The solo strip (rfd_device.cuh) computes each cell's geometry on the step-to-step
 // dependency chain, so a sparse band - a handful of live lanes per step - advances at the
 // latency of two FP64 quadratics per step.  Here the geometry leaves that chain:
-//   warps 1..3 (helpers)  compute a whole skewed 32x32 tile of step-chunk c - for the
+//   warps 1..7 (helpers)  compute a whole skewed 32x32 tile of step-chunk c - for the
 //                          decision the right and top free intervals of every cell, for
 //                          VE-FD the two vertex-edge weights - into shared memory;
 //   warp 0 (propagator)   runs the same skewed sweep, the same L2 strip handoff and the
@@ -11,7 +11,8 @@
 //                          shared-memory read, two shuffles and the min/max propagation.
 // Tile c+1 is requested speculatively while tile c is consumed (two slots, mbarrier
 // handshakes); a jump cancels the speculative tile.  The arithmetic of every cell is the
-// solo strip's (same functions), so results are bit-identical.
+// solo strip's (same functions), so results are bit-identical.  The same code, instantiated
+// with MIR, sweeps the mirror half of a split pair from the far corner (mirror_interval).
 #pragma once
 
 #include <type_traits>
@@ -121,7 +122,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
   }
 }
 
-// ------------------------------------------------------------------ helpers (warps 1..3)
+// ------------------------------------------------------------------ helpers (warps 1..H)
 
 // Mirror sweep (MIR, meet in the middle): the grid seen from its far corner.  Mirror cell
 // (i, j) is cell (a, b) = (mrow - i, C - 1 - j) of the pair, and its tile holds the values of
