@@ -44,13 +44,17 @@ WORKLOAD = ("long pair: 2 x 200,000-point 3D spline paths (2,000 waypoints U[-10
             "20-knot time warp, noise 0.1, seed 1); FD to 2^-33 relative")
 # algorithmic FP64 flops per cell (fma = 2, sqrt/div = 1), from the reference expressions:
 # DFD .cu:615-626, VE-FD .cu:373-419, decision .cu:1173-1244
-DEC_DRAM_BYTES_20K = 3.730432e6   # ncu, one decision launch of the 20,000-point case
-VEFD_DRAM_BYTES_20K = 4.31e6      # ncu, one VE-FD launch of the same case (two launches averaged)
+# ncu dram__bytes_read.sum + dram__bytes_write.sum on the 20,000-point case: one decision
+# round, both halves of the split pair (mirror 3.584768 MB + forward 4.161792 MB); one VE-FD
+# launch of the unsplit pair (two launches averaged; the split VE-FD was not captured)
+DEC_DRAM_BYTES_20K = 3.584768e6 + 4.161792e6
+VEFD_DRAM_BYTES_20K = 4.31e6
 COARSE_UB = 6  # the learned form's upper bound: inflated DFD of every 6th point (rfd.h coarse_ub)
 ARITY = 4  # batched forms: radii per round for the longest-chain pairs (rfd.h search_arity)
 DFD_DRAM_BYTES_200K = 31.5e6 + 68.4e6  # ncu, the exact DFD launch of the long pair (32-row ring)
 KERNEL_OF_PHASE = {"dfd": f"dfd_kernel<{'1, INFL' if COARSE_UB else '8'}>",
-                   "vefd": "team_kernel<K_VEFD>", "search": "team_kernel<K_DEC>"}
+                   "vefd": "team_kernel<K_VEFD> (forward and mirror halves)",
+                   "search": "team_kernel<K_DEC> (forward and mirror halves)"}
 FLOPS_PER_CELL = {"dfd": lambda d: 3 * d + 3 + (4 if COARSE_UB else 0),  # + sqrt, 2 adds, square
                   "vefd": lambda d: 24 * d + 2,
                   "search": lambda d: 12 * d + 22}
@@ -690,8 +694,11 @@ def main():
                      "flops_per_cell": FLOPS_PER_CELL[dom](d), "cells": cells[dom],
                      "traffic_note": ("bytes per launch, ncu capture of the full-size launch"
                                       if dom == "dfd" else
-                                      "bytes per launch, ncu cold-cache capture at 20k points "
-                                      "scaled by points")},
+                                      "bytes per probe round (both halves of the split pair), "
+                                      "ncu cold-cache capture at 20k points scaled by points"
+                                      if dom == "search" else
+                                      "bytes of one unsplit VE-FD launch, ncu cold-cache capture "
+                                      "at 20k points scaled by points")},
         # the pruned sweeps are bound by their dependency chain, not by flops or bytes: the
         # wavefront has n1 + n2 anti-diagonals, so this is the latency each one adds
         "critical_path": {
