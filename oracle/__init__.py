@@ -56,6 +56,8 @@ def lib():
         L.rfd_oracle_search.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_int, _dp, _ip]
+        L.rfd_oracle_split.argtypes = [ctypes.c_int, _dp, i64, _dp, i64, ctypes.c_int,
+                                       ctypes.c_double, i64, _dp]
         L.rfd_oracle_max_threads.restype = ctypes.c_int
         L.rfd_verify_decision.restype = ctypes.c_int
         L.rfd_verify_decision.argtypes = [_dp, i64, _dp, i64, ctypes.c_int, ctypes.c_double]
@@ -125,6 +127,18 @@ def decide(P, Q, radius, threads=1, formula=0):
     if rc:
         raise RuntimeError(f"oracle decide failed ({rc})")
     return out.value == 1.0, out.value
+
+
+def split(kind, P, Q, x, h):
+    """Meet in the middle at row h (see rfd_oracle_split): kind 1 the squared VE-FD seeded
+    by x, kind 2 the decision at radius x (1.0 reachable, -2.0 not)."""
+    P, Q = _arr(P), _arr(Q)
+    out = ctypes.c_double()
+    rc = lib().rfd_oracle_split(kind, _ptr(P), len(P), _ptr(Q), len(Q), P.shape[1], x, h,
+                                ctypes.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle split failed ({rc})")
+    return out.value
 
 
 FLT_EPSILON = float(np.finfo(np.float32).eps)

@@ -451,6 +451,136 @@ int rfd_oracle_free_intervals(int64_t n, const double* x, const double* a, const
   return rfd_oracle_free_intervals_formula(n, x, a, b, A, inv2A, r2, d, 0, lo, hi);
 }
 
+/* Meet in the middle, restated (the CUDA engine's split pairs: split_meet_kernel and the
+   mirror instantiation of the team strips, robotfd_b200/csrc/).  The decision or VE-FD DP of
+   rows 0 .. h-1 runs forward from the start as above; rows h .. R-1 run from the far corner
+   over the mirrored grid, whose cell (i, j) is cell (a, b) = (R-1-i, C-1-j) carrying that
+   cell's entry edges - the right edge of cell (a-1, b) (p_a against q_b q_{b+1}) and the top
+   edge of cell (a, b-1) (q_b against p_a p_{a+1}) - with the same propagation rule: VE-FD
+   weights as they are, starting from min(w_top, w_right) of the last cell; free intervals
+   [lo, hi] as [-hi, -lo] (empty (-3, -4), dead below -1.5), starting from the last cell's
+   right edge when its interval reaches the corner (upper end 1.0).  The two rows handed
+   across the boundary between rows h-1 and h then combine:
+     K_VEFD: *out = min over b of max(forward(b), mirror(C-1-b)), the squared VE-FD;
+     K_DEC:  *out = 1.0 if some b has forward(b) >= 0, mirror(C-1-b) >= -1.5 and
+             forward(b) <= -mirror(C-1-b), else -2.0.
+   Sequential; checks on real geometry that the split equals the unsplit DP (VE-FD bit for
+   bit, reachable iff the unsplit right UB is 1.0).  x is the radius (K_DEC) or the lower
+   bound seeding VE-FD (K_VEFD); 1 <= h <= R-1. */
+static void mirror_iv(double* lo, double* hi) {
+  if (*lo < 0.0) {
+    *lo = -3.0;
+    *hi = -4.0;
+  } else {
+    double l = *lo;
+    *lo = -*hi;
+    *hi = -l;
+  }
+}
+
+int rfd_oracle_split(int kind, const double* P, int64_t n1, const double* Q, int64_t n2, int d,
+                     double x, int64_t h, double* out) {
+  if (kind != K_VEFD && kind != K_DEC) return -1;
+  const int64_t R = n1 - 1, C = n2 - 1;
+  if (R < 2 || C < 1 || d < 1 || d > 3 || h < 1 || h > R - 1) return -1;
+  ora_t o;
+  memset(&o, 0, sizeof(o));
+  o.kind = kind;
+  o.d = d;
+  o.P = P;
+  o.Q = Q;
+  o.r2 = kind == K_DEC ? x * x : 0.0;
+  o.seed = kind == K_VEFD ? x * x : 0.0;
+  o.R = h; /* the forward half: rows 0 .. h-1 */
+  o.C = C;
+  if (prep_segments(P, n1, d, &o.rowA, &o.rowInv) || prep_segments(Q, n2, d, &o.colA, &o.colInv))
+    return -2;
+  o.down = (double*)malloc(sizeof(double) * C);
+  o.bot = (double*)malloc(sizeof(double) * h);
+  double* M = (double*)malloc(sizeof(double) * C);
+  if (!o.down || !o.bot || !M) return -2;
+  for (int64_t j = 0; j < C; ++j) o.down[j] = kind == K_DEC ? -1.0 : ORA_FLTMAX;
+  for (int64_t i = 0; i < h; ++i) {
+    if (kind == K_DEC) o.bot[i] = i == 0 ? 0.0 : -1.0;
+    else o.bot[i] = i == 0 ? o.seed : ORA_FLTMAX;
+  }
+  tile(&o, 0, h, 0, C); /* o.down: the values handed from row h-1 to row h */
+  const double* Pl = P + R * d;        /* p_R, the last point */
+  const double* Ql = Q + C * d;        /* q_C */
+  /* the far corner */
+  double bm0;
+  if (kind == K_VEFD) {
+    const double wr = pt_seg_sq(Pl, Q + (C - 1) * d, Ql, o.colA[C - 1], d);
+    const double wt = pt_seg_sq(Ql, P + (R - 1) * d, Pl, o.rowA[R - 1], d);
+    bm0 = cmin(wt, wr);
+    for (int64_t j = 0; j < C; ++j) M[j] = ORA_FLTMAX;
+  } else {
+    double lo, hi;
+    free_interval(Pl, Q + (C - 1) * d, Ql, o.colA[C - 1], o.colInv[C - 1], o.r2, d, 0, &lo, &hi);
+    for (int64_t j = 0; j < C; ++j) M[j] = -3.0;
+    if (hi == 1.0) M[0] = -1.0;
+    bm0 = -3.0;
+  }
+  for (int64_t i = 0; i < R - h; ++i) {
+    const int64_t a = R - 1 - i;
+    const double* pa = P + a * d;
+    const double* pa1 = P + (a + 1) * d;
+    double bm = i == 0 ? bm0 : (kind == K_DEC ? -3.0 : ORA_FLTMAX);
+    for (int64_t jm = 0; jm < C; ++jm) {
+      const int64_t b = C - 1 - jm;
+      const double* qb = Q + b * d;
+      const double* qb1 = Q + (b + 1) * d;
+      if (kind == K_VEFD) {
+        const double in = cmin(M[jm], bm);
+        const double wr = pt_seg_sq(pa, qb, qb1, o.colA[b], d);      /* p_a vs q_b q_{b+1} */
+        const double wt = pt_seg_sq(qb, pa, pa1, o.rowA[a], d);      /* q_b vs p_a p_{a+1} */
+        const double top = cmax(wt, in), right = cmax(wr, in);
+        M[jm] = right;
+        bm = top;
+      } else {
+        double rLB, rUB, tLB, tUB;
+        free_interval(pa, qb, qb1, o.colA[b], o.colInv[b], o.r2, d, 0, &rLB, &rUB);
+        free_interval(qb, pa, pa1, o.rowA[a], o.rowInv[a], o.r2, d, 0, &tLB, &tUB);
+        mirror_iv(&rLB, &rUB);
+        mirror_iv(&tLB, &tUB);
+        const double left = M[jm];
+        if (bm < -1.5) {
+          const int invalid = (left > rUB) || (left < -1.5);
+          const double m = cmax(rLB, left);
+          rLB = invalid ? -3.0 : m;
+        }
+        if (left < -1.5) {
+          const int invalid = (bm > tUB) || (bm < -1.5);
+          const double m = cmax(tLB, bm);
+          tLB = invalid ? -3.0 : m;
+        }
+        bm = tLB;
+        M[jm] = rLB;
+      }
+    }
+  }
+  if (kind == K_VEFD) {
+    double v = ORA_FLTMAX;
+    for (int64_t b = 0; b < C; ++b) v = cmin(v, cmax(o.down[b], M[C - 1 - b]));
+    *out = v;
+  } else {
+    int found = 0;
+    for (int64_t b = 0; b < C && !found; ++b) {
+      const double f = o.down[b], m = M[C - 1 - b];
+      found = f >= 0.0 && m >= -1.5 && f <= -m;
+    }
+    *out = found ? 1.0 : -2.0;
+  }
+  free(M);
+  free(o.down);
+  free(o.bot);
+  free(o.rowA);
+  free(o.rowInv);
+  free(o.colA);
+  free(o.colInv);
+  return 0;
+}
+
 int rfd_oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();
