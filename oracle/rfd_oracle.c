@@ -16,6 +16,8 @@
  *                                 boundaries .cu:1026-1027 (start) and .cu:656 (left edge -1)
  *   - epsilon search              src/frechet.cpp:36-63, eps = FLT_EPSILON
  *                                 (src/compute_distance_wrapper.cpp:6); VE-FD launch rule .cu:1343
+ *   - and, with no reference counterpart, the CUDA engine's meet in the middle
+ *     (rfd_oracle_split), to check on the CPU that it gives the unsplit DPs' results
  *
  * Arithmetic contract (shared bit for bit with the CUDA kernels): FP64, compiled with
  * -ffp-contract=off, restating the reference kernels as nvcc compiles them (default
