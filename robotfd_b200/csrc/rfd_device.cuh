@@ -83,9 +83,9 @@ struct PairDesc {
   // the right and top edges exchanged
   int n1, n2, d, tr;
   // Meet in the middle (team strips of one pair, run_batch): the forward sweep of a split pair
-  // runs its first `split` strips only; the pair's mirror descriptor (split = -1) sweeps the
-  // rest of the grid from the far corner, its row r being row mrow - r of the pair's grid
-  // (n1 then counts the mirror's rows + 1).  0 for every other descriptor.
+  // runs its first `split` strips only; the pair's mirror descriptor (split = -(p + 1) for
+  // pair p) sweeps the rest of the grid from the far corner, its row r being row mrow - r of
+  // the pair's grid (n1 then counts the mirror's rows + 1).  0 for every other descriptor.
   int split, mrow;
   long long cstride, tstride;
 };
